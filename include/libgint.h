@@ -1,0 +1,103 @@
+/*
+ * libgint.h -- C-ABI of the B200 exchange-matrix (K) engine.
+ *
+ * Drop-in for the libGint C-ABI used by CP2K's HFX_LIBRARY libGint path: the same symbol
+ * names, argument meanings and call protocol as the reference's src/extern_functions.cpp
+ * (cited per entry point below), all wrapped around one opaque handle. Plain pointers and
+ * sizes only. Contract summary (identical to the reference unless stated):
+ *
+ *   setup   libgint_create_handle, libgint_init, libgint_set_Potential_Truncated,
+ *           libgint_set_hf_fac, libgint_set_max_mem, libgint_set_cell, libgint_set_neighs,
+ *           libgint_set_Atom / libgint_set_Atom_L for every basis set
+ *   K build libgint_set_P (zeroes K) ; per set quartet:
+ *             [ libgint_add_prm* libgint_add_shell ]*   (one add_shell per image pair n1,n2)
+ *             libgint_add_qrt ; libgint_add_qrtt*       (contractions in lexicographic order)
+ *             libgint_add_set
+ *           libgint_get_K  (K accumulated as K_bd += -f I_abcd P_ac, ... ; f = symm_fac*hf_fac)
+ *
+ * Differences from the reference, all additive:
+ *   - errors never terminate the process; they are recorded and read with libgint_last_error;
+ *   - libgint_destroy_handle releases a handle;
+ *   - libgint_set_precision / libgint_get_stats / libgint_rebuild_K are extensions.
+ * Threading: one handle per host thread; handles are independent (each owns its stream and
+ * device buffers), so the reference's team-collective calls need no omp barrier here.
+ */
+#ifndef LIBGINT_B200_H
+#define LIBGINT_B200_H
+
+#include <stdbool.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* src/extern_functions.cpp:9   new engine handle */
+void *libgint_create_handle(void);
+/* src/extern_functions.cpp:17  binds the handle to the current CUDA device and a stream */
+void libgint_init(void *handle);
+/* src/extern_functions.cpp:22  truncated Coulomb with cutoff R_cut (bohr); C0 is the
+ * per-patch Chebyshev table, ld_C0 = (nder+1)*105 doubles per patch, C0_size total doubles */
+void libgint_set_Potential_Truncated(void *handle, double R_cut, double *C0, int ld_C0, int C0_size);
+/* src/extern_functions.cpp:27  K += -hf_fac * ... */
+void libgint_set_hf_fac(void *handle, double fac);
+/* src/extern_functions.cpp:34  device memory budget in MB for work buffers */
+void libgint_set_max_mem(void *handle, int max_mem);
+/* src/extern_functions.cpp:40  copies P (P_size doubles) to the device and zeroes K */
+void libgint_set_P(void *handle, double *P, int P_size);
+/* src/extern_functions.cpp:46  spin-polarised variant (P_alpha, P_beta) */
+void libgint_set_P_polarized(void *handle, double *Pa, double *Pb, int P_size);
+/* src/extern_functions.cpp:52  initial value of K */
+void libgint_set_K(void *handle, double *K, int K_size);
+/* src/extern_functions.cpp:57 */
+void libgint_set_K_polarized(void *handle, double *Ka, double *Kb, int K_size);
+/* src/extern_functions.cpp:62  completes all queued work and copies K to the host */
+void libgint_get_K(void *handle, double *K);
+/* src/extern_functions.cpp:67 */
+void libgint_get_K_polarized(void *handle, double *Ka, double *Kb);
+/* src/extern_functions.cpp:72  cell_h: rows are lattice vectors (bohr); cell_i its inverse */
+void libgint_set_cell(void *handle, bool periodic, double *cell_h, double *cell_i);
+/* src/extern_functions.cpp:77  nneighs lattice vectors (3 doubles each), nneighs <= 256 */
+void libgint_set_neighs(void *handle, double *neighs, int nneighs);
+/* src/extern_functions.cpp:82  set i: centre R[3], np <= 16 exponents Z */
+void libgint_set_Atom(void *handle, int i, double *R, double *Z, int np);
+/* src/extern_functions.cpp:114 set i: nl <= 4 contractions of angular momentum l <= 3,
+ * K[nl*np]; coefficients are renormalised as in the reference */
+void libgint_set_Atom_L(void *handle, int i, int l, int nl, double *K);
+/* src/extern_functions.cpp:139 */
+void libgint_set_AtomInfo(void *handle, int i, double *R, double *Z, int np, int lmin, int Lmax,
+                          int *nl, double *K);
+/* src/extern_functions.cpp:149 one surviving primitive quartet (indices within each set) */
+void libgint_add_prm(void *handle, int ipa, int ipb, int ipc, int ipd);
+/* src/extern_functions.cpp:154 sets i,j,k,l with images n1 (of b) and n2 (of d) */
+void libgint_add_shell(void *handle, int i, int j, int k, int l, int n1, int n2);
+/* src/extern_functions.cpp:159 no-op */
+void libgint_add_cell(void *handle);
+/* src/extern_functions.cpp:164 */
+void libgint_add_qrt(void *handle, int la, int lb, int lc, int ld, int nla, int nlb, int nlc, int nld);
+/* src/extern_functions.cpp:169 one contraction combination; symm_fac in {2,1,0.5,0.25,0};
+ * ld_* < 256; offsets index the caller's P/K arrays; T* choose the transposed walk */
+void libgint_add_qrtt(void *handle, double symm_fac, int la, int lb, int lc, int ld,
+                      int inla, int inlb, int inlc, int inld,
+                      int ld_ac, int ld_ad, int ld_bc, int ld_bd,
+                      unsigned int offset_ac_L_set, unsigned int offset_ad_L_set,
+                      unsigned int offset_bc_L_set, unsigned int offset_bd_L_set,
+                      bool Tac, bool Tad, bool Tbc, bool Tbd);
+/* src/extern_functions.cpp:182 closes the set quartet */
+void libgint_add_set(void *handle);
+/* src/extern_functions.cpp:187 launches all queued work */
+void libgint_dispatch(void *handle);
+
+/* ---- extensions (no counterpart in the reference's C-ABI) ------------------------------- */
+/* last error code of the handle (0 = none); the text is returned by libgint_error_string */
+int libgint_last_error(void *handle);
+const char *libgint_error_string(void *handle);
+void libgint_destroy_handle(void *handle);
+/* sizes of the recursion plan of class (la,lb,lc,ld): out[0..7] = VRR workspace, contracted
+ * targets, HRR workspace (doubles), cartesian and spherical block sizes, VRR blocks, HRR
+ * steps, primitive team size; returns 0 for an unsupported class */
+int libgint_plan_sizes(int la, int lb, int lc, int ld, int *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,739 @@
+// engine.cpp -- host engine and C-ABI of the B200 K build.
+//
+// The caller streams screened quartets through the libgint_* calls exactly as for the
+// reference (src/libGint.cpp:151-414). The engine keeps one host queue per angular-momentum
+// class; add_set commits a set quartet as one group record (all its image pairs and
+// contraction rows). When the queues reach the work-buffer budget they are flushed: packed
+// class-sorted into one pinned staging buffer, copied with one cudaMemcpyAsync, and processed
+// by two kernels per class on the handle's stream. Two staging/device slots alternate, so the
+// GPU works on one batch while the caller fills the next. get_K drains the queue and copies K.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/libgint.h"
+#include "engine_types.h"
+#include "kernels.h"
+#include "tcg_patches.h"
+
+namespace gint {
+
+// ---------------------------------------------------------------------------------------
+// tables built on the host
+// ---------------------------------------------------------------------------------------
+// Boys table F_m(T), T = 0, 0.1, ..., 12.0 and m = 0..27 (the Taylor table of the
+// reference's fgamma0, src/fgamma.cpp:109-123), from the convergent series
+// F_m(T) = exp(-T) sum_k (2T)^k / ((2m+1)(2m+3)...(2m+2k+1)) in extended precision.
+static void make_boys_table(std::vector<double> &ft) {
+   ft.assign(121 * 28, 0.0);
+   for (int it = 0; it <= 120; it++) {
+      long double T = (long double)it * 0.1L;
+      for (int m = 0; m < 28; m++) {
+         long double term = 1.0L / (2 * m + 1), sum = term;
+         for (int k = 1; k < 400; k++) {
+            term *= 2.0L * T / (2 * m + 2 * k + 1);
+            sum += term;
+            if (term < 1e-22L * sum) break;
+         }
+         ft[it * 28 + m] = (double)(std::exp(-T) * sum);
+      }
+   }
+}
+
+// Cartesian -> real solid harmonic coefficients in CP2K's order and normalisation (the
+// values of the reference's src/c2s.h): unnormalised solid harmonics, each row scaled to
+// the norm of the monomial x^.. with unit exponents, l = 3 rows rounded to 9 decimals as in
+// the CP2K table.
+static void make_c2s(double out[4][70]) {
+   static const int sh1[3][3] = {{0, 1, 0}, {0, 0, 1}, {1, 0, 0}};
+   static const int sh2[5][6] = {{0, 1, 0, 0, 0, 0}, {0, 0, 0, 0, 1, 0}, {-1, 0, 0, -1, 0, 2},
+                                 {0, 0, 1, 0, 0, 0}, {1, 0, 0, -1, 0, 0}};
+   static const int sh3[7][10] = {{0, 3, 0, 0, 0, 0, -1, 0, 0, 0}, {0, 0, 0, 0, 1, 0, 0, 0, 0, 0},
+                                  {0, -1, 0, 0, 0, 0, -1, 0, 4, 0}, {0, 0, -3, 0, 0, 0, 0, -3, 0, 2},
+                                  {-1, 0, 0, -1, 0, 4, 0, 0, 0, 0}, {0, 0, 1, 0, 0, 0, 0, -1, 0, 0},
+                                  {1, 0, 0, -3, 0, 0, 0, 0, 0, 0}};
+   auto df = [](int n) { double r = 1; for (int k = n; k > 1; k -= 2) r *= k; return r; };
+   auto exps = [](int l, int i, int e[3]) {
+      int a = 0; while ((a + 1) * (a + 2) / 2 <= i) a++;
+      e[0] = l - a; e[2] = i - a * (a + 1) / 2; e[1] = a - e[2];
+   };
+   std::memset(out, 0, sizeof(double) * 4 * 70);
+   out[0][0] = 1.0;
+   for (int l = 1; l <= 3; l++) {
+      int nc = (l + 1) * (l + 2) / 2;
+      for (int m = 0; m < 2 * l + 1; m++) {
+         const int *row = l == 1 ? sh1[m] : (l == 2 ? sh2[m] : sh3[m]);
+         double n2 = 0;
+         for (int i = 0; i < nc; i++) for (int j = 0; j < nc; j++) {
+            if (!row[i] || !row[j]) continue;
+            int e1[3], e2[3]; exps(l, i, e1); exps(l, j, e2);
+            double o = 1;
+            for (int d = 0; d < 3; d++) { int s = e1[d] + e2[d]; if (s & 1) { o = 0; break; } o *= df(s - 1); }
+            n2 += row[i] * row[j] * o;
+         }
+         double nr = std::sqrt(n2);
+         for (int i = 0; i < nc; i++) {
+            double v = row[i] / nr;
+            if (l >= 3) v = std::round(v * 1e9) / 1e9;
+            out[l][m * nc + i] = v;
+         }
+      }
+   }
+}
+
+// ---------------------------------------------------------------------------------------
+// handle
+// ---------------------------------------------------------------------------------------
+struct HostSet {
+   double R[3] = {0, 0, 0};
+   int np = 0;
+   double Z[kMaxPrm] = {0};
+   int nL = 0;
+   int l[8] = {0}, nl[8] = {0};
+   std::vector<double> K[8];
+   bool defined = false;
+};
+
+struct PendShell { int cls; uint32_t ent[4]; uint16_t n1, n2; uint32_t prm_off, nprm; };
+struct PendQrt { int cls; uint8_t nl[4]; };
+struct PendQrtt { int cls; QrttRec rec; };
+
+struct ClassQ {
+   std::vector<uint32_t> prm, prm_shell;
+   std::vector<ShellRec> shells;
+   std::vector<GroupRec> groups;
+   std::vector<QrttRec> qrtts;
+   bool active = false;
+};
+
+struct DBuf {
+   void *p = nullptr;
+   size_t bytes = 0;
+};
+
+struct Slot {
+   char *h_stage = nullptr;
+   size_t stage_bytes = 0;
+   DBuf rec, ac, gscr;
+   cudaEvent_t ev = nullptr;
+   bool busy = false;
+};
+
+struct Handle {
+   int device = 0;
+   cudaStream_t stream = nullptr;
+   int err = 0;
+   std::string errmsg;
+   // potential and tables
+   double R_cut = 0;
+   std::vector<double> C0;
+   int ld_C0 = 0;
+   bool have_pot = false, pot_dirty = true;
+   double hf_fac = 1.0;
+   size_t max_mem_mb = 4000;
+   bool periodic = false;
+   double cell[18] = {0};
+   std::vector<double> neighs{0.0, 0.0, 0.0};
+   int Ng = 1;
+   bool neighs_dirty = true;
+   // basis
+   std::vector<HostSet> sets;
+   std::vector<int> ent_base;
+   bool basis_dirty = true, ent_dirty = true;
+   // device-resident data
+   DBuf d_pool, d_ents, d_neighs, d_C0, d_lut, d_bw, d_ft, d_plans, d_err;
+   DBuf d_P[2], d_K[2];
+   int nspin = 0;
+   size_t FP_size = 0;
+   ClassPlan plans[256];
+   bool plans_ready = false;
+   // streaming state
+   std::vector<uint32_t> prm_tmp;
+   std::vector<PendShell> set_shells;
+   std::vector<uint32_t> set_prms;
+   std::vector<PendQrt> set_qrts;
+   std::vector<PendQrtt> set_qrtts;
+   ClassQ q[256];
+   std::vector<int> active;
+   size_t pend_prims = 0, pend_ac = 0, pend_rec = 0;
+   Slot slots[2];
+   int cur = 0;
+   // statistics
+   long long n_shells = 0, n_prims = 0, n_groups = 0, n_flush = 0;
+};
+
+static void set_error(Handle *h, int code, const std::string &msg) {
+   if (!h->err) { h->err = code; h->errmsg = msg; }
+}
+
+static bool ck(Handle *h, cudaError_t e, const char *what) {
+   if (e == cudaSuccess) return true;
+   set_error(h, 100 + (int)e, std::string(what) + ": " + cudaGetErrorString(e));
+   return false;
+}
+
+static bool ensure(Handle *h, DBuf &b, size_t bytes, const char *what) {
+   if (b.bytes >= bytes && b.p) return true;
+   if (b.p) { cudaFree(b.p); b.p = nullptr; b.bytes = 0; }
+   size_t alloc = std::max<size_t>(bytes, 256);
+   if (!ck(h, cudaMalloc(&b.p, alloc), what)) return false;
+   b.bytes = alloc;
+   return true;
+}
+
+static void release(DBuf &b) { if (b.p) cudaFree(b.p); b.p = nullptr; b.bytes = 0; }
+
+static inline int cls_of(int la, int lb, int lc, int ld) { return la * 64 + lb * 16 + lc * 4 + ld; }
+
+static void ensure_ent_base(Handle *h);
+
+static bool upload_tables(Handle *h) {
+   if (h->err) return false;
+   ensure_ent_base(h);
+   if (!h->plans_ready) {
+      if (!ensure(h, h->d_plans, sizeof(ClassPlan) * 256, "plans")) return false;
+      if (!ck(h, cudaMemcpy(h->d_plans.p, h->plans, sizeof(ClassPlan) * 256, cudaMemcpyHostToDevice), "plans")) return false;
+      // patch maps and (bias, weight) per patch from the rectangle table
+      std::vector<uint8_t> lut(2 * 128 * 128);
+      for (int i1 = 0; i1 < 128; i1++) {
+         double X1 = (double)i1 / 127.0;
+         for (int i2 = 0; i2 < 128; i2++) {
+            double X2 = (double)i2 / 127.0;
+            for (int side = 0; side < 2; side++) {
+               int first = side ? TCG_NPATCH_LOW : 0, last = side ? TCG_NPATCH : TCG_NPATCH_LOW;
+               int found = 0;
+               for (int p = first; p < last; p++) {
+                  double lo1 = tcg_patch_rect[p][0] / 128.0, hi1 = tcg_patch_rect[p][1] / 128.0;
+                  double lo2 = tcg_patch_rect[p][2] / 128.0, hi2 = tcg_patch_rect[p][3] / 128.0;
+                  bool in1 = X1 <= hi1 && (X1 > lo1 || lo1 == 0.0);
+                  bool in2 = X2 <= hi2 && (X2 > lo2 || lo2 == 0.0);
+                  if (in1 && in2) { found = p; break; }
+               }
+               lut[side * 128 * 128 + i1 * 128 + i2] = (uint8_t)found;
+            }
+         }
+      }
+      std::vector<double> bw(TCG_NPATCH * 4);
+      for (int p = 0; p < TCG_NPATCH; p++) {
+         bw[p * 4 + 0] = (tcg_patch_rect[p][0] + tcg_patch_rect[p][1]) / 128.0;
+         bw[p * 4 + 1] = 128.0 / (tcg_patch_rect[p][1] - tcg_patch_rect[p][0]);
+         bw[p * 4 + 2] = (tcg_patch_rect[p][2] + tcg_patch_rect[p][3]) / 128.0;
+         bw[p * 4 + 3] = 128.0 / (tcg_patch_rect[p][3] - tcg_patch_rect[p][2]);
+      }
+      std::vector<double> ft;
+      make_boys_table(ft);
+      if (!ensure(h, h->d_lut, lut.size(), "lut") || !ensure(h, h->d_bw, bw.size() * 8, "bw") ||
+          !ensure(h, h->d_ft, ft.size() * 8, "ftable") || !ensure(h, h->d_err, sizeof(int) * 4, "err"))
+         return false;
+      if (!ck(h, cudaMemcpy(h->d_lut.p, lut.data(), lut.size(), cudaMemcpyHostToDevice), "lut")) return false;
+      if (!ck(h, cudaMemcpy(h->d_bw.p, bw.data(), bw.size() * 8, cudaMemcpyHostToDevice), "bw")) return false;
+      if (!ck(h, cudaMemcpy(h->d_ft.p, ft.data(), ft.size() * 8, cudaMemcpyHostToDevice), "ftable")) return false;
+      if (!ck(h, cudaMemset(h->d_err.p, 0, sizeof(int) * 4), "err")) return false;
+      double c2s[4][70];
+      make_c2s(c2s);
+      const double symm[5] = {2.0, 1.0, 0.5, 0.25, 0.0};
+      if (!ck(h, upload_constant_tables(&c2s[0][0], symm), "constant tables")) return false;
+      h->plans_ready = true;
+   }
+   if (h->basis_dirty) {
+      std::vector<double> pool;
+      std::vector<BasisEnt> ents;
+      for (size_t s = 0; s < h->sets.size(); s++) {
+         const HostSet &hs = h->sets[s];
+         int zoff = (int)pool.size();
+         pool.insert(pool.end(), hs.Z, hs.Z + hs.np);
+         for (int e = 0; e < hs.nL; e++) {
+            BasisEnt be;
+            std::memset(&be, 0, sizeof(be));
+            for (int q = 0; q < 3; q++) be.R[q] = hs.R[q];
+            be.z_off = zoff; be.np = hs.np; be.nl = hs.nl[e]; be.l = hs.l[e];
+            be.k_off = (int)pool.size();
+            pool.insert(pool.end(), hs.K[e].begin(), hs.K[e].end());
+            ents.push_back(be);
+         }
+      }
+      if (pool.empty()) pool.push_back(0.0);
+      if (ents.empty()) ents.push_back(BasisEnt{});
+      if (!ensure(h, h->d_pool, pool.size() * 8, "basis") || !ensure(h, h->d_ents, ents.size() * sizeof(BasisEnt), "basis"))
+         return false;
+      if (!ck(h, cudaMemcpy(h->d_pool.p, pool.data(), pool.size() * 8, cudaMemcpyHostToDevice), "basis")) return false;
+      if (!ck(h, cudaMemcpy(h->d_ents.p, ents.data(), ents.size() * sizeof(BasisEnt), cudaMemcpyHostToDevice), "basis")) return false;
+      h->basis_dirty = false;
+   }
+   if (h->pot_dirty && h->have_pot) {
+      if (!ensure(h, h->d_C0, h->C0.size() * 8, "C0")) return false;
+      if (!ck(h, cudaMemcpy(h->d_C0.p, h->C0.data(), h->C0.size() * 8, cudaMemcpyHostToDevice), "C0")) return false;
+      h->pot_dirty = false;
+   }
+   if (h->neighs_dirty) {
+      if (!ensure(h, h->d_neighs, h->neighs.size() * 8, "neighs")) return false;
+      if (!ck(h, cudaMemcpy(h->d_neighs.p, h->neighs.data(), h->neighs.size() * 8, cudaMemcpyHostToDevice), "neighs")) return false;
+      h->neighs_dirty = false;
+   }
+   return true;
+}
+
+static void ensure_ent_base(Handle *h) {
+   if (h->ent_base.size() == h->sets.size() && !h->ent_dirty) return;
+   h->ent_base.assign(h->sets.size(), 0);
+   int n = 0;
+   for (size_t s = 0; s < h->sets.size(); s++) { h->ent_base[s] = n; n += h->sets[s].nL; }
+   h->ent_dirty = false;
+}
+
+static DevCtx make_ctx(Handle *h) {
+   DevCtx c;
+   std::memset(&c, 0, sizeof(c));
+   c.pool = (const double *)h->d_pool.p;
+   c.ents = (const BasisEnt *)h->d_ents.p;
+   c.neighs = (const double *)h->d_neighs.p;
+   c.Ng = h->Ng;
+   c.nspin = h->nspin;
+   std::memcpy(c.cell, h->cell, sizeof(c.cell));
+   c.R_cut = h->R_cut;
+   c.C0 = (const double *)h->d_C0.p;
+   c.ld_C0 = h->ld_C0;
+   c.lut_low = (const uint8_t *)h->d_lut.p;
+   c.lut_high = (const uint8_t *)h->d_lut.p + 128 * 128;
+   c.bw = (const double *)h->d_bw.p;
+   c.ftable = (const double *)h->d_ft.p;
+   for (int s = 0; s < 2; s++) { c.P[s] = (const double *)h->d_P[s].p; c.K[s] = (double *)h->d_K[s].p; }
+   c.hf_fac = h->hf_fac;
+   c.FP_size = h->FP_size;
+   c.err = (int *)h->d_err.p;
+   return c;
+}
+
+static size_t slot_budget_bytes(Handle *h) {
+   // two slots share ~90% of the caller's budget
+   return std::max<size_t>((size_t)h->max_mem_mb * 1024 * 1024 * 9 / 20, 64u << 20);
+}
+
+static inline size_t al16(size_t x) { return (x + 15) & ~(size_t)15; }
+
+static void flush(Handle *h) {
+   if (h->active.empty()) return;
+   if (h->err) { // drop queued work after an error
+      for (int c : h->active) { ClassQ &Q = h->q[c]; Q.prm.clear(); Q.prm_shell.clear(); Q.shells.clear(); Q.groups.clear(); Q.qrtts.clear(); Q.active = false; }
+      h->active.clear(); h->pend_prims = h->pend_ac = h->pend_rec = 0;
+      return;
+   }
+   if (!upload_tables(h)) return;
+   if (h->nspin == 0 || !h->d_K[0].p) { set_error(h, 4, "work queued before libgint_set_P"); return; }
+   if (!h->have_pot) { set_error(h, 4, "work queued before libgint_set_Potential_Truncated"); return; }
+   for (int c : h->active) {
+      if (h->ld_C0 < (h->plans[c].L + 1) * 105) {
+         set_error(h, 2, "C0 holds fewer derivative orders than la+lb+lc+ld+1");
+         return;
+      }
+   }
+   Slot &s = h->slots[h->cur];
+   h->cur ^= 1;
+   if (s.busy) { ck(h, cudaEventSynchronize(s.ev), "slot wait"); s.busy = false; }
+   // layout of the staging buffer: per class, prm | prm_shell | shells | groups | qrtts
+   struct Seg { int c; size_t o_prm, o_ps, o_sh, o_g, o_q; size_t ac_off; };
+   std::vector<Seg> segs;
+   size_t off = 0, ac = 0;
+   for (int c : h->active) {
+      ClassQ &Q = h->q[c];
+      Seg g;
+      g.c = c;
+      g.o_prm = off; off = al16(off + Q.prm.size() * 4);
+      g.o_ps = off; off = al16(off + Q.prm_shell.size() * 4);
+      g.o_sh = off; off = al16(off + Q.shells.size() * sizeof(ShellRec));
+      g.o_g = off; off = al16(off + Q.groups.size() * sizeof(GroupRec));
+      g.o_q = off; off = al16(off + Q.qrtts.size() * sizeof(QrttRec));
+      g.ac_off = ac;
+      ac += ((size_t)Q.prm.size() * h->plans[c].S + 1) & ~(size_t)1;
+      segs.push_back(g);
+   }
+   if (s.stage_bytes < off) {
+      if (s.h_stage) cudaFreeHost(s.h_stage);
+      s.h_stage = nullptr; s.stage_bytes = 0;
+      size_t want = std::max(off, (size_t)(64u << 20));
+      if (!ck(h, cudaHostAlloc((void **)&s.h_stage, want, cudaHostAllocPortable), "pinned staging")) return;
+      s.stage_bytes = want;
+   }
+   if (!ensure(h, s.rec, std::max(off, (size_t)(64u << 20)), "record buffer")) return;
+   if (!ensure(h, s.ac, std::max(ac * 8, (size_t)(64u << 20)), "AC buffer")) return;
+   for (const Seg &g : segs) {
+      ClassQ &Q = h->q[g.c];
+      std::memcpy(s.h_stage + g.o_prm, Q.prm.data(), Q.prm.size() * 4);
+      std::memcpy(s.h_stage + g.o_ps, Q.prm_shell.data(), Q.prm_shell.size() * 4);
+      std::memcpy(s.h_stage + g.o_sh, Q.shells.data(), Q.shells.size() * sizeof(ShellRec));
+      std::memcpy(s.h_stage + g.o_g, Q.groups.data(), Q.groups.size() * sizeof(GroupRec));
+      std::memcpy(s.h_stage + g.o_q, Q.qrtts.data(), Q.qrtts.size() * sizeof(QrttRec));
+   }
+   if (!ck(h, cudaMemcpyAsync(s.rec.p, s.h_stage, off, cudaMemcpyHostToDevice, h->stream), "record upload")) return;
+   DevCtx ctx = make_ctx(h);
+   for (const Seg &g : segs) {
+      ClassQ &Q = h->q[g.c];
+      const ClassPlan &hp = h->plans[g.c];
+      BatchArgs bt;
+      std::memset(&bt, 0, sizeof(bt));
+      char *base = (char *)s.rec.p;
+      bt.plan = (const ClassPlan *)h->d_plans.p + g.c;
+      bt.prm = (const uint32_t *)(base + g.o_prm);
+      bt.prm_shell = (const uint32_t *)(base + g.o_ps);
+      bt.shells = (const ShellRec *)(base + g.o_sh);
+      bt.groups = (const GroupRec *)(base + g.o_g);
+      bt.qrtts = (const QrttRec *)(base + g.o_q);
+      bt.nprm = (uint32_t)Q.prm.size();
+      bt.nshell = (uint32_t)Q.shells.size();
+      bt.ngroup = (uint32_t)Q.groups.size();
+      bt.AC = (double *)s.ac.p + g.ac_off;
+      int gg = 0, gw = 0;
+      size_t gs = group_global_scratch(hp, &gg, &gw);
+      if (gs) {
+         if (!ensure(h, s.gscr, gs * 8, "HRR scratch")) return;
+         bt.gscratch = (double *)s.gscr.p;
+      }
+      if (!ck(h, launch_prim(ctx, bt, hp, h->stream), "k_prim launch")) return;
+      if (!ck(h, launch_group(ctx, bt, hp, h->stream), "k_group launch")) return;
+      h->n_prims += bt.nprm; h->n_shells += bt.nshell; h->n_groups += bt.ngroup;
+      Q.prm.clear(); Q.prm_shell.clear(); Q.shells.clear(); Q.groups.clear(); Q.qrtts.clear();
+      Q.active = false;
+   }
+   h->active.clear();
+   h->pend_prims = h->pend_ac = h->pend_rec = 0;
+   ck(h, cudaEventRecord(s.ev, h->stream), "event record");
+   s.busy = true;
+   h->n_flush++;
+}
+
+static void drain(Handle *h) {
+   flush(h);
+   ck(h, cudaStreamSynchronize(h->stream), "stream synchronize");
+   if (h->d_err.p && !h->err) {
+      int e = 0;
+      if (ck(h, cudaMemcpy(&e, h->d_err.p, sizeof(int), cudaMemcpyDeviceToHost), "error flag") && e)
+         set_error(h, 3, "a K update addressed P/K outside P_size");
+   }
+}
+
+static void set_P_impl(Handle *h, int nspin, const double *Pa, const double *Pb, int n) {
+   if (n <= 0) { set_error(h, 2, "P_size must be positive"); return; }
+   // the previous build must be complete before P/K are replaced
+   for (Slot &s : h->slots) if (s.busy) { ck(h, cudaEventSynchronize(s.ev), "slot wait"); s.busy = false; }
+   ck(h, cudaStreamSynchronize(h->stream), "stream synchronize");
+   h->nspin = nspin;
+   h->FP_size = (size_t)n;
+   const double *src[2] = {Pa, Pb};
+   for (int sp = 0; sp < nspin; sp++) {
+      if (!ensure(h, h->d_P[sp], (size_t)n * 8, "P") || !ensure(h, h->d_K[sp], (size_t)n * 8, "K")) return;
+      if (!ck(h, cudaMemcpy(h->d_P[sp].p, src[sp], (size_t)n * 8, cudaMemcpyHostToDevice), "P upload")) return;
+      if (!ck(h, cudaMemsetAsync(h->d_K[sp].p, 0, (size_t)n * 8, h->stream), "K zero")) return;
+   }
+   upload_tables(h);
+}
+
+static void get_K_impl(Handle *h, double *Ka, double *Kb) {
+   drain(h);
+   if (h->nspin == 0) { set_error(h, 4, "libgint_get_K before libgint_set_P"); return; }
+   double *dst[2] = {Ka, Kb};
+   for (int sp = 0; sp < h->nspin; sp++)
+      if (dst[sp]) ck(h, cudaMemcpy(dst[sp], h->d_K[sp].p, h->FP_size * 8, cudaMemcpyDeviceToHost), "K download");
+}
+
+}  // namespace gint
+
+using namespace gint;
+
+// ---------------------------------------------------------------------------------------
+// C-ABI (reference src/extern_functions.cpp:9-190)
+// ---------------------------------------------------------------------------------------
+extern "C" {
+
+void *libgint_create_handle(void) {
+   Handle *h = new Handle();
+   for (int c = 0; c < 256; c++) build_class_plan(c >> 6, (c >> 4) & 3, (c >> 2) & 3, c & 3, h->plans[c]);
+   return h;
+}
+
+void libgint_init(void *hh) {
+   Handle *h = (Handle *)hh;
+   ck(h, cudaGetDevice(&h->device), "cudaGetDevice");
+   if (!h->stream) ck(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream");
+   for (Slot &s : h->slots) if (!s.ev) ck(h, cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming), "event");
+}
+
+void libgint_set_Potential_Truncated(void *hh, double R_cut, double *C0, int ld_C0, int C0_size) {
+   Handle *h = (Handle *)hh;
+   if (!C0 || ld_C0 < 105 || ld_C0 % 105 != 0 || C0_size < 207 * ld_C0) {
+      set_error(h, 2, "libgint_set_Potential_Truncated: C0 must hold 207 patches of ld_C0 = (nder+1)*105 doubles");
+      return;
+   }
+   h->R_cut = R_cut;
+   h->ld_C0 = ld_C0;
+   h->C0.assign(C0, C0 + C0_size);
+   h->have_pot = true;
+   h->pot_dirty = true;
+}
+
+void libgint_set_hf_fac(void *hh, double fac) { ((Handle *)hh)->hf_fac = fac; }
+
+void libgint_set_max_mem(void *hh, int max_mem) {
+   Handle *h = (Handle *)hh;
+   if (max_mem > 0) h->max_mem_mb = (size_t)max_mem;
+}
+
+void libgint_set_P(void *hh, double *P, int P_size) { set_P_impl((Handle *)hh, 1, P, nullptr, P_size); }
+
+void libgint_set_P_polarized(void *hh, double *Pa, double *Pb, int P_size) { set_P_impl((Handle *)hh, 2, Pa, Pb, P_size); }
+
+void libgint_set_K(void *hh, double *K, int K_size) {
+   Handle *h = (Handle *)hh;
+   if (h->nspin < 1 || (size_t)K_size != h->FP_size) { set_error(h, 2, "libgint_set_K: call set_P first with the same size"); return; }
+   drain(h);
+   ck(h, cudaMemcpy(h->d_K[0].p, K, (size_t)K_size * 8, cudaMemcpyHostToDevice), "K upload");
+}
+
+void libgint_set_K_polarized(void *hh, double *Ka, double *Kb, int K_size) {
+   Handle *h = (Handle *)hh;
+   if (h->nspin < 2 || (size_t)K_size != h->FP_size) { set_error(h, 2, "libgint_set_K_polarized: call set_P_polarized first"); return; }
+   drain(h);
+   ck(h, cudaMemcpy(h->d_K[0].p, Ka, (size_t)K_size * 8, cudaMemcpyHostToDevice), "K upload");
+   ck(h, cudaMemcpy(h->d_K[1].p, Kb, (size_t)K_size * 8, cudaMemcpyHostToDevice), "K upload");
+}
+
+void libgint_get_K(void *hh, double *K) { get_K_impl((Handle *)hh, K, nullptr); }
+
+void libgint_get_K_polarized(void *hh, double *Ka, double *Kb) { get_K_impl((Handle *)hh, Ka, Kb); }
+
+void libgint_set_cell(void *hh, bool periodic, double *cell_h, double *cell_i) {
+   Handle *h = (Handle *)hh;
+   h->periodic = periodic;   // stored; the wrap always uses the cell, as in the reference
+   for (int i = 0; i < 9; i++) { h->cell[i] = cell_h[i]; h->cell[9 + i] = cell_i[i]; }
+}
+
+void libgint_set_neighs(void *hh, double *neighs, int nneighs) {
+   Handle *h = (Handle *)hh;
+   if (nneighs < 1 || nneighs > kMaxCell) { set_error(h, 2, "libgint_set_neighs: 1 <= nneighs <= 256"); return; }
+   h->neighs.assign(neighs, neighs + 3 * (size_t)nneighs);
+   h->Ng = nneighs;
+   h->neighs_dirty = true;
+}
+
+void libgint_set_Atom(void *hh, int i, double *R, double *Z, int np) {
+   Handle *h = (Handle *)hh;
+   if (i < 0 || np < 1 || np > kMaxPrm) { set_error(h, 2, "libgint_set_Atom: 1 <= np <= 16"); return; }
+   if ((size_t)i >= h->sets.size()) h->sets.resize(i + 1);
+   HostSet &s = h->sets[i];
+   s = HostSet();
+   for (int q = 0; q < 3; q++) s.R[q] = R[q];
+   s.np = np;
+   for (int p = 0; p < np; p++) s.Z[p] = Z[p];
+   s.defined = true;
+   h->basis_dirty = true;
+   h->ent_dirty = true;
+}
+
+void libgint_set_Atom_L(void *hh, int i, int l, int nl, double *K) {
+   Handle *h = (Handle *)hh;
+   if (i < 0 || (size_t)i >= h->sets.size() || !h->sets[i].defined) { set_error(h, 2, "libgint_set_Atom_L: set not defined"); return; }
+   if (l < 0 || l > kMaxL || nl < 1 || nl > kMaxNl) { set_error(h, 2, "libgint_set_Atom_L: l <= 3 and 1 <= nl <= 4"); return; }
+   HostSet &s = h->sets[i];
+   if (s.nL >= 8) { set_error(h, 2, "libgint_set_Atom_L: too many l entries in one set"); return; }
+   const int np = s.np;
+   std::vector<double> Kn((size_t)nl * np);
+   for (int c = 0; c < nl; c++) {
+      // renormalisation of the reference (src/extern_functions.cpp:95-136)
+      const double *Kr = K + (size_t)c * np;
+      double ans = 0.0;
+      for (int a = 0; a < np; a++) for (int b = 0; b < np; b++) ans += Kr[a] * Kr[b] / std::pow(s.Z[a] + s.Z[b], 1.5 + l);
+      ans *= std::pow(M_PI, 1.5) / std::pow(2.0, l);
+      double nrm = std::sqrt(ans);
+      for (int p = 0; p < np; p++) Kn[(size_t)c * np + p] = Kr[p] / nrm;
+   }
+   s.l[s.nL] = l; s.nl[s.nL] = nl; s.K[s.nL] = Kn; s.nL++;
+   h->basis_dirty = true;
+   h->ent_dirty = true;
+}
+
+void libgint_set_AtomInfo(void *hh, int i, double *R, double *Z, int np, int lmin, int Lmax, int *nl, double *K) {
+   libgint_set_Atom(hh, i, R, Z, np);
+   int k_offset = 0;
+   for (int l = lmin; l < Lmax; l++) {
+      libgint_set_Atom_L(hh, i, l, nl[l - lmin], &K[k_offset]);
+      k_offset += nl[l - lmin] * np;
+   }
+}
+
+void libgint_add_prm(void *hh, int ipa, int ipb, int ipc, int ipd) {
+   Handle *h = (Handle *)hh;
+   h->prm_tmp.push_back(((uint32_t)ipa << 24) | ((uint32_t)ipb << 16) | ((uint32_t)ipc << 8) | (uint32_t)ipd);
+}
+
+void libgint_add_shell(void *hh, int i, int j, int k, int l, int n1, int n2) {
+   Handle *h = (Handle *)hh;
+   if (h->prm_tmp.empty()) return;
+   const int ns = (int)h->sets.size();
+   if (i < 0 || j < 0 || k < 0 || l < 0 || i >= ns || j >= ns || k >= ns || l >= ns || n1 < 0 || n2 < 0 ||
+       n1 >= h->Ng || n2 >= h->Ng) {
+      set_error(h, 2, "libgint_add_shell: set or image index out of range");
+      h->prm_tmp.clear();
+      return;
+   }
+   ensure_ent_base(h);
+   const HostSet *S4[4] = {&h->sets[i], &h->sets[j], &h->sets[k], &h->sets[l]};
+   const int idx[4] = {i, j, k, l};
+   for (uint32_t p : h->prm_tmp) {
+      if ((int)(p >> 24) >= S4[0]->np || (int)((p >> 16) & 255) >= S4[1]->np || (int)((p >> 8) & 255) >= S4[2]->np ||
+          (int)(p & 255) >= S4[3]->np) {
+         set_error(h, 2, "libgint_add_prm: primitive index out of range");
+         h->prm_tmp.clear();
+         return;
+      }
+   }
+   const uint32_t poff = (uint32_t)h->set_prms.size();
+   const uint32_t np = (uint32_t)h->prm_tmp.size();
+   h->set_prms.insert(h->set_prms.end(), h->prm_tmp.begin(), h->prm_tmp.end());
+   h->prm_tmp.clear();
+   for (int a = 0; a < S4[0]->nL; a++) for (int b = 0; b < S4[1]->nL; b++)
+   for (int c = 0; c < S4[2]->nL; c++) for (int d = 0; d < S4[3]->nL; d++) {
+      PendShell ps;
+      ps.cls = cls_of(S4[0]->l[a], S4[1]->l[b], S4[2]->l[c], S4[3]->l[d]);
+      const int li[4] = {a, b, c, d};
+      for (int q = 0; q < 4; q++) ps.ent[q] = (uint32_t)(h->ent_base[idx[q]] + li[q]);
+      ps.n1 = (uint16_t)n1; ps.n2 = (uint16_t)n2;
+      ps.prm_off = poff; ps.nprm = np;
+      h->set_shells.push_back(ps);
+   }
+}
+
+void libgint_add_cell(void *hh) { (void)hh; }
+
+void libgint_add_qrt(void *hh, int la, int lb, int lc, int ld, int nla, int nlb, int nlc, int nld) {
+   Handle *h = (Handle *)hh;
+   if (la < 0 || lb < 0 || lc < 0 || ld < 0 || la > kMaxL || lb > kMaxL || lc > kMaxL || ld > kMaxL ||
+       nla < 1 || nlb < 1 || nlc < 1 || nld < 1 || nla > kMaxNl || nlb > kMaxNl || nlc > kMaxNl || nld > kMaxNl) {
+      set_error(h, 2, "libgint_add_qrt: l <= 3 and 1 <= nl <= 4");
+      return;
+   }
+   PendQrt q;
+   q.cls = cls_of(la, lb, lc, ld);
+   q.nl[0] = (uint8_t)nla; q.nl[1] = (uint8_t)nlb; q.nl[2] = (uint8_t)nlc; q.nl[3] = (uint8_t)nld;
+   h->set_qrts.push_back(q);
+}
+
+void libgint_add_qrtt(void *hh, double symm_fac, int la, int lb, int lc, int ld, int inla, int inlb, int inlc, int inld,
+                      int ld_ac, int ld_ad, int ld_bc, int ld_bd, unsigned int off_ac, unsigned int off_ad,
+                      unsigned int off_bc, unsigned int off_bd, bool Tac, bool Tad, bool Tbc, bool Tbd) {
+   Handle *h = (Handle *)hh;
+   (void)inla; (void)inlb; (void)inlc; (void)inld;
+   if (ld_ac < 0 || ld_ad < 0 || ld_bc < 0 || ld_bd < 0 || ld_ac > 255 || ld_ad > 255 || ld_bc > 255 || ld_bd > 255) {
+      set_error(h, 2, "libgint_add_qrtt: leading dimensions must be < 256");
+      return;
+   }
+   // symmetry factor encoding of the reference (src/libGint.cpp:262-267)
+   unsigned idx_fac = 0;
+   if (symm_fac < 0.1) idx_fac = 4;
+   else if (symm_fac < 0.3) idx_fac = 3;
+   else if (symm_fac < 0.75) idx_fac = 2;
+   else if (symm_fac < 1.5) idx_fac = 1;
+   PendQrtt q;
+   q.cls = cls_of(la, lb, lc, ld);
+   q.rec.off[0] = off_ac; q.rec.off[1] = off_ad; q.rec.off[2] = off_bc; q.rec.off[3] = off_bd;
+   q.rec.ld[0] = (uint8_t)ld_ac; q.rec.ld[1] = (uint8_t)ld_ad; q.rec.ld[2] = (uint8_t)ld_bc; q.rec.ld[3] = (uint8_t)ld_bd;
+   q.rec.T = (uint8_t)((Tac ? 1 : 0) | (Tad ? 2 : 0) | (Tbc ? 4 : 0) | (Tbd ? 8 : 0));
+   q.rec.idx_fac = (uint8_t)idx_fac;
+   q.rec.pad[0] = q.rec.pad[1] = 0;
+   h->set_qrtts.push_back(q);
+}
+
+void libgint_add_set(void *hh) {
+   Handle *h = (Handle *)hh;
+   for (const PendQrt &pq : h->set_qrts) {
+      ClassQ &Q = h->q[pq.cls];
+      GroupRec g;
+      g.shell_off = (uint32_t)Q.shells.size();
+      g.nshell = 0;
+      g.qrtt_off = (uint32_t)Q.qrtts.size();
+      for (int q = 0; q < 4; q++) g.nl[q] = pq.nl[q];
+      const uint32_t gid = (uint32_t)Q.groups.size();
+      size_t added_prims = 0;
+      for (const PendShell &ps : h->set_shells) {
+         if (ps.cls != pq.cls) continue;
+         ShellRec sr;
+         for (int q = 0; q < 4; q++) sr.ent[q] = ps.ent[q];
+         sr.prm_off = (uint32_t)Q.prm.size();
+         sr.nprm = ps.nprm;
+         sr.n1 = ps.n1; sr.n2 = ps.n2;
+         sr.group = gid;
+         const uint32_t sid = (uint32_t)Q.shells.size();
+         Q.prm.insert(Q.prm.end(), h->set_prms.begin() + ps.prm_off, h->set_prms.begin() + ps.prm_off + ps.nprm);
+         Q.prm_shell.insert(Q.prm_shell.end(), ps.nprm, sid);
+         Q.shells.push_back(sr);
+         g.nshell++;
+         added_prims += ps.nprm;
+      }
+      const int nrows = pq.nl[0] * pq.nl[1] * pq.nl[2] * pq.nl[3];
+      int nq = 0;
+      for (const PendQrtt &pt : h->set_qrtts) {
+         if (pt.cls != pq.cls) continue;
+         if (nq < nrows) Q.qrtts.push_back(pt.rec);
+         nq++;
+      }
+      if (g.nshell == 0 || nq != nrows) {
+         // nothing to compute, or an inconsistent set: roll back this group
+         if (g.nshell && nq != nrows) set_error(h, 2, "libgint_add_set: add_qrtt count differs from nla*nlb*nlc*nld");
+         Q.prm.resize(Q.prm.size() - added_prims);
+         Q.prm_shell.resize(Q.prm_shell.size() - added_prims);
+         Q.shells.resize(g.shell_off);
+         Q.qrtts.resize(g.qrtt_off);
+         continue;
+      }
+      Q.groups.push_back(g);
+      if (!Q.active) { Q.active = true; h->active.push_back(pq.cls); }
+      const int S = h->plans[pq.cls].S;
+      h->pend_prims += added_prims;
+      h->pend_ac += added_prims * (size_t)S;
+      h->pend_rec += added_prims * 8 + g.nshell * sizeof(ShellRec) + sizeof(GroupRec) + nrows * sizeof(QrttRec);
+   }
+   h->set_shells.clear();
+   h->set_prms.clear();
+   h->set_qrts.clear();
+   h->set_qrtts.clear();
+   const size_t budget = slot_budget_bytes(h);
+   if (h->pend_ac * 8 > budget * 7 / 10 || h->pend_rec > budget * 3 / 10) flush(h);
+}
+
+void libgint_dispatch(void *hh) { flush((Handle *)hh); }
+
+int libgint_last_error(void *hh) { return ((Handle *)hh)->err; }
+
+// Sizes of the recursion plan of one class (VRR workspace, contracted targets, HRR workspace,
+// cartesian and spherical block sizes), for inspection and tests.
+int libgint_plan_sizes(int la, int lb, int lc, int ld, int *out) {
+   ClassPlan p;
+   if (!build_class_plan(la, lb, lc, ld, p)) return 0;
+   out[0] = p.V; out[1] = p.S; out[2] = p.H; out[3] = p.Nc; out[4] = p.Ns; out[5] = p.nvb; out[6] = p.nhop;
+   out[7] = prim_team_size(p);
+   return 1;
+}
+
+const char *libgint_error_string(void *hh) { return ((Handle *)hh)->errmsg.c_str(); }
+
+void libgint_destroy_handle(void *hh) {
+   Handle *h = (Handle *)hh;
+   if (!h) return;
+   if (h->stream) cudaStreamSynchronize(h->stream);
+   for (Slot &s : h->slots) {
+      if (s.h_stage) cudaFreeHost(s.h_stage);
+      release(s.rec); release(s.ac); release(s.gscr);
+      if (s.ev) cudaEventDestroy(s.ev);
+   }
+   DBuf *bufs[] = {&h->d_pool, &h->d_ents, &h->d_neighs, &h->d_C0, &h->d_lut, &h->d_bw, &h->d_ft,
+                   &h->d_plans, &h->d_err, &h->d_P[0], &h->d_P[1], &h->d_K[0], &h->d_K[1]};
+   for (DBuf *b : bufs) release(*b);
+   if (h->stream) cudaStreamDestroy(h->stream);
+   delete h;
+}
+
+}  // extern "C"

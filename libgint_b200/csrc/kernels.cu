@@ -1,0 +1,625 @@
+// kernels.cu -- sm_100a kernels of the K build.
+//
+// Two kernels per angular-momentum class (la,lb,lc,ld), launched on class-sorted segments of
+// one batch:
+//
+//  k_prim<TS>   one team of TS lanes per primitive quartet. The lanes evaluate the images n3
+//               in parallel (truncated-Coulomb G_m by the patch Chebyshev series, or the Boys
+//               function), drop screened images, then run the Obara-Saika VRR of each
+//               surviving image cooperatively, level by level, in the team's shared-memory
+//               workspace, and sum the (e0|f0)^(0) targets over n3. The image-summed targets
+//               of the primitive go to the AC buffer.
+//               (reference: src/compute_Fm.cpp:20-326, src/compute_VRR.cpp:349-458,
+//                src/compute_ECO.cpp:216-272)
+//  k_group      one warp per group (all image pairs of one set quartet for one class): for
+//               every contraction row, contract AC over the primitives of each shell, apply
+//               the HRR with that shell's AB/CD, sum the shells, transform to spherical and
+//               update K with atomics.
+//               (reference: src/compute_ECO.cpp:12-214, src/compute_HRR.cpp:102-225,
+//                src/compute_SPH.cpp:58-237, src/compute_KS.cpp:8-117)
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cstdint>
+#include "engine_types.h"
+#include "kernels.h"
+
+namespace gint {
+
+__constant__ int8_t c_cart_exp[8][36][3];
+__constant__ int8_t c_cart_dir[8][36];
+__constant__ int8_t c_cart_dec[8][36][3];
+__constant__ int8_t c_cart_inc[8][36][3];
+__constant__ double c_c2s[4][70];
+__constant__ double c_symm[5];
+
+static __device__ __forceinline__ int ncart(int l) { return (l + 1) * (l + 2) / 2; }
+
+// ---------------------------------------------------------------------------------------
+// Boys function (reference src/fgamma.cpp:196-243), result scaled by fac
+// ---------------------------------------------------------------------------------------
+static __device__ void boys_eval(int nmax, double T, double *f, const double *__restrict__ ft, double fac) {
+   if (T < 1.e-13) {
+      for (int n = 0; n <= nmax; n++) f[n] = fac / (2. * n + 1.);
+      return;
+   }
+   if (T < 12.) {
+      const double tdelta = 0.1;
+      int itab = (int)(round(T / tdelta));
+      double ttab = (double)itab * tdelta;
+      const double *row = ft + itab * 28 + nmax;
+      double d = ttab - T, tmp = d;
+      double fL = __ldg(row + 0);
+      fL += __ldg(row + 1) * tmp;
+      tmp *= d; fL += __ldg(row + 2) * tmp * 0.5;
+      tmp *= d; fL += __ldg(row + 3) * tmp * (1. / 6.);
+      tmp *= d; fL += __ldg(row + 4) * tmp * (1. / 24.);
+      tmp *= d; fL += __ldg(row + 5) * tmp * (1. / 120.);
+      tmp *= d; fL += __ldg(row + 6) * tmp * (1. / 720.);
+      double expt = exp(-T);
+      f[nmax] = fL;
+      for (int n = nmax - 1; n >= 0; n--) f[n] = (2.0 * T * f[n + 1] + expt) / (2. * n + 1.);
+   } else {
+      double tmp = 1.0 / T, tmp2 = tmp * tmp, tmp3 = tmp * tmp2;
+      double g = 0.4999489092 - 0.2473631686 * tmp + 0.321180909 * tmp2 - 0.3811559346 * tmp3;
+      double expt = exp(-T);
+      f[0] = 0.5 * sqrt(M_PI * tmp) - g * expt * tmp;
+      for (int n = 1; n <= nmax; n++) f[n] = (0.5 * tmp) * ((2. * n - 1.) * f[n - 1] - expt);
+   }
+   for (int n = 0; n <= nmax; n++) f[n] *= fac;
+}
+
+// ---------------------------------------------------------------------------------------
+// Truncated-Coulomb G_m(T,R) * Kfac (reference src/t_c_g0_n.cpp:67-180); falls back to the
+// Boys function for R > 11 and T < R^2 - 11 R.
+// ---------------------------------------------------------------------------------------
+static __device__ void fm_eval(const DevCtx &ctx, int L, double R, double T, double Kfac, double *res) {
+   double upper = R * R + 11.0 * R + 50.0;
+   double lower = R * R - 11.0 * R + 0.0;
+   double X1, X2;
+   int patch;
+   if (T > upper) {
+      for (int n = 0; n <= L; n++) res[n] = 0.0;
+      return;
+   }
+   if (R <= 11.0) {
+      X2 = R / 11.0;
+      upper = R * R + 11.0 * R + 50.0;
+      lower = 0.0;
+      X1 = (T - lower) / (upper - lower);
+      int i1 = (int)(X1 * 128), i2 = (int)(X2 * 128);
+      if (i1 == 128) i1 = 127;
+      if (i2 == 128) i2 = 127;
+      patch = __ldg(ctx.lut_low + i1 * 128 + i2);
+   } else {
+      if (T < lower) {
+         boys_eval(L, T, res, ctx.ftable, Kfac);
+         return;
+      }
+      X2 = 11.0 / R;
+      X1 = (T - lower) / (upper - lower);
+      int i1 = (int)(X1 * 128), i2 = (int)(X2 * 128);
+      if (i1 == 128) i1 = 127;
+      if (i2 == 128) i2 = 127;
+      patch = __ldg(ctx.lut_high + i1 * 128 + i2);
+   }
+   const double B1 = __ldg(ctx.bw + patch * 4 + 0), W1 = __ldg(ctx.bw + patch * 4 + 1);
+   const double B2 = __ldg(ctx.bw + patch * 4 + 2), W2 = __ldg(ctx.bw + patch * 4 + 3);
+   const double *C0_row = ctx.C0 + (size_t)ctx.ld_C0 * patch;
+   const double SQ2 = 1.4142135623730950488016887242096980785696718753;
+   double TG1 = (2. * X1 - B1) * W1;
+   double TG2 = (2. * X2 - B2) * W2;
+   double T1[14], T2[14];
+   T1[0] = 1.0; T2[0] = 1.0;
+   T1[1] = SQ2 * TG1; T2[1] = SQ2 * TG2;
+   T1[2] = 2. * TG1 * T1[1] - SQ2; T2[2] = 2. * TG2 * T2[1] - SQ2;
+#pragma unroll
+   for (int i = 3; i < 14; i++) {
+      T1[i] = 2. * TG1 * T1[i - 1] - T1[i - 2];
+      T2[i] = 2. * TG2 * T2[i - 1] - T2[i - 2];
+   }
+   for (int k = 0; k <= L; k++) {
+      const double *c = C0_row + k * 105;
+      double tmp = 0.0;
+      int jl = 0;
+#pragma unroll
+      for (int j = 0; j < 14; j++) {
+         double dot = 0.0;
+#pragma unroll
+         for (int l = 0; l < 14 - j; l++) { dot += T1[l] * __ldg(c + jl); jl++; }
+         tmp += dot * T2[j];
+      }
+      res[k] = tmp * Kfac;
+   }
+}
+
+// minimum-image wrap (reference src/util.cpp:235-265)
+static __device__ __forceinline__ void pbc(const double *A, const double *B, const double *cell, double *AB) {
+   const double *hm = cell, *hi = cell + 9;
+   AB[0] = B[0] - A[0]; AB[1] = B[1] - A[1]; AB[2] = B[2] - A[2];
+   double s0 = hi[0] * AB[0] + hi[3] * AB[1] + hi[6] * AB[2];
+   double s1 = hi[1] * AB[0] + hi[4] * AB[1] + hi[7] * AB[2];
+   double s2 = hi[2] * AB[0] + hi[5] * AB[1] + hi[8] * AB[2];
+   s0 -= round(s0); s1 -= round(s1); s2 -= round(s2);
+   AB[0] = hm[0] * s0 + hm[3] * s1 + hm[6] * s2;
+   AB[1] = hm[1] * s0 + hm[4] * s1 + hm[7] * s2;
+   AB[2] = hm[2] * s0 + hm[5] * s1 + hm[8] * s2;
+}
+
+// shell geometry: A, B (image n1), C, D (image n2) as the reference places them
+static __device__ __forceinline__ void shell_geom(const DevCtx &ctx, const BasisEnt &ea, const BasisEnt &eb,
+                                                  const BasisEnt &ec, const BasisEnt &ed, int n1, int n2,
+                                                  double *A, double *B, double *C, double *D, double *CDs) {
+   double ABs[3];
+   pbc(ea.R, eb.R, ctx.cell, ABs);
+   pbc(ec.R, ed.R, ctx.cell, CDs);
+   for (int q = 0; q < 3; q++) {
+      A[q] = ea.R[q];
+      B[q] = ea.R[q] + ABs[q] + __ldg(ctx.neighs + n1 * 3 + q);
+      C[q] = ec.R[q];
+      D[q] = ec.R[q] + CDs[q] + __ldg(ctx.neighs + n2 * 3 + q);
+   }
+}
+
+// ---------------------------------------------------------------------------------------
+// One VRR element of block b (reference VRR1..VRR6, src/compute_VRR.cpp:111-345)
+// pqz: PA[3] WP[3] QC[3] WQ[3] i2ab mrab i2cd mrcd i2z
+// ---------------------------------------------------------------------------------------
+static __device__ __forceinline__ void vrr_elem(const VBlock &b, int e, double *ws, const double *pqz) {
+   const int a = b.a, c = b.c;
+   const int na = ncart(a), nc = ncart(c);
+   const int k = e % nc, i = (e / nc) % na, mm = e / (nc * na);
+   const int m = b.lo + mm;
+   double v;
+   if (c == 0) {
+      const int d = c_cart_dir[a][i];
+      const int im = c_cart_dec[a][i][d];
+      const int na1 = ncart(a - 1);
+      const double *b1 = ws + b.in1;
+      v = pqz[d] * b1[(m - b.lo1) * na1 + im] + pqz[3 + d] * b1[(m + 1 - b.lo1) * na1 + im];
+      const int ed = c_cart_exp[a][i][d];
+      if (ed >= 2) {
+         const int iw = c_cart_dec[a - 1][im][d];
+         const int na2 = ncart(a - 2);
+         const double *b2 = ws + b.in2;
+         v += (ed - 1) * (pqz[12] * b2[(m - b.lo2) * na2 + iw] + pqz[13] * b2[(m + 1 - b.lo2) * na2 + iw]);
+      }
+   } else {
+      const int d = c_cart_dir[c][k];
+      const int km = c_cart_dec[c][k][d];
+      const int nc1 = ncart(c - 1);
+      const double *b1 = ws + b.in1;
+      v = pqz[6 + d] * b1[((m - b.lo1) * na + i) * nc1 + km] + pqz[9 + d] * b1[((m + 1 - b.lo1) * na + i) * nc1 + km];
+      const int cd = c_cart_exp[c][k][d];
+      if (cd >= 2) {
+         const int kw = c_cart_dec[c - 1][km][d];
+         const int nc2 = ncart(c - 2);
+         const double *b2 = ws + b.in2;
+         v += (cd - 1) * (pqz[14] * b2[((m - b.lo2) * na + i) * nc2 + kw] + pqz[15] * b2[((m + 1 - b.lo2) * na + i) * nc2 + kw]);
+      }
+      if (a > 0) {
+         const int ad = c_cart_exp[a][i][d];
+         if (ad >= 1) {
+            const int im = c_cart_dec[a][i][d];
+            const double *b3 = ws + b.in3;
+            v += ad * pqz[16] * b3[((m + 1 - b.lo3) * ncart(a - 1) + im) * nc1 + km];
+         }
+      }
+   }
+   ws[b.off + e] = v;
+}
+
+template <int TS>
+static __device__ __forceinline__ void team_sync(unsigned mask) {
+   if (TS > 1) __syncwarp(mask);
+}
+
+// ---------------------------------------------------------------------------------------
+// k_prim: Fm + VRR + sum over n3 per primitive quartet
+// ---------------------------------------------------------------------------------------
+template <int TS>
+__global__ void __launch_bounds__(256) k_prim(DevCtx ctx, BatchArgs bt, int team_doubles) {
+   extern __shared__ __align__(16) double smem[];
+   ClassPlan *pl = reinterpret_cast<ClassPlan *>(smem);
+   {
+      const int nwords = (int)(sizeof(ClassPlan) / 4);
+      const int *src = reinterpret_cast<const int *>(bt.plan);
+      int *dst = reinterpret_cast<int *>(smem);
+      for (int w = threadIdx.x; w < nwords; w += blockDim.x) dst[w] = src[w];
+   }
+   __syncthreads();
+   const int plan_doubles = (int)((sizeof(ClassPlan) + 15) / 16) * 2;
+   const int team = threadIdx.x / TS, lane = threadIdx.x % TS, nteam = blockDim.x / TS;
+   double *tws = smem + plan_doubles + (size_t)team * team_doubles;
+   const int L = pl->L, V = pl->V, S = pl->S;
+   double *ws = tws;                  // VRR workspace [V]
+   double *acc = tws + V;             // image-summed targets [S]
+   double *pqz = acc + S;             // 17 factors of the image being processed
+   double *fmx = pqz + 17;            // per-lane Fm [TS][L+1]
+   const unsigned wl = (threadIdx.x & 31) / TS * TS;
+   const unsigned mask = (TS >= 32) ? 0xffffffffu : (((1u << TS) - 1u) << wl);
+
+   for (uint32_t p = blockIdx.x * nteam + team; p < bt.nprm; p += gridDim.x * nteam) {
+      const uint32_t code = bt.prm[p];
+      const ShellRec sh = bt.shells[bt.prm_shell[p]];
+      const BasisEnt ea = ctx.ents[sh.ent[0]], eb = ctx.ents[sh.ent[1]];
+      const BasisEnt ec = ctx.ents[sh.ent[2]], ed = ctx.ents[sh.ent[3]];
+      const int ipa = code >> 24, ipb = (code >> 16) & 255, ipc = (code >> 8) & 255, ipd = code & 255;
+      double A[3], B[3], C[3], D[3], CDs[3];
+      shell_geom(ctx, ea, eb, ec, ed, sh.n1, sh.n2, A, B, C, D, CDs);
+      const double za = ctx.pool[ea.z_off + ipa], zb = ctx.pool[eb.z_off + ipb];
+      const double zc = ctx.pool[ec.z_off + ipc], zd = ctx.pool[ed.z_off + ipd];
+      // prepare_Fm (reference src/compute_Fm.cpp:66-159)
+      const double zab = za + zb, inv_zab = 1. / zab, zcd = zc + zd, inv_zcd = 1. / zcd;
+      const double z = zab + zcd, inv_z = 1. / z;
+      double P[3], Q[3], PQs[3], shift[3];
+      for (int q = 0; q < 3; q++) {
+         P[q] = (za * A[q] + zb * B[q]) * inv_zab;
+         Q[q] = (zc * C[q] + zd * D[q]) * inv_zcd;
+      }
+      pbc(Q, P, ctx.cell, PQs);
+      for (int q = 0; q < 3; q++) shift[q] = P[q] - Q[q] - PQs[q];
+      const double normf = 2. * 17.493418327624862 * inv_zab * inv_zcd;   // 2 pi^(5/2) / (zab zcd)
+      double dx = A[0] - B[0], dy = A[1] - B[1], dz = A[2] - B[2];
+      const double RAB2 = dx * dx + dy * dy + dz * dz;
+      const double expon_ab = -(za * zb) / (za + zb) * RAB2;
+      dx = C[0] - D[0]; dy = C[1] - D[1]; dz = C[2] - D[2];
+      const double RCD2 = dx * dx + dy * dy + dz * dz;
+      const double expon_cd = -(zc * zd) / (zc + zd) * RCD2;
+      const double Kfac = (1. / sqrt(z)) * normf * exp(expon_ab + expon_cd);
+      double Cs[3], Ds[3];
+      for (int q = 0; q < 3; q++) {
+         Cs[q] = C[q] + shift[q];
+         Ds[q] = C[q] + CDs[q] + __ldg(ctx.neighs + sh.n2 * 3 + q) + shift[q];
+      }
+      for (int q = 0; q < 3; q++) Q[q] = (zc * Cs[q] + zd * Ds[q]) * inv_zcd;
+      const double rho = zab * zcd * inv_z;
+      const double R = ctx.R_cut * sqrt(rho);
+      const double izab = 1. / zab, i2ab = 0.5 * izab, mrab = -1. * rho * izab * i2ab;
+      const double izcd = 1. / zcd, i2cd = 0.5 * izcd, mrcd = -1. * rho * izcd * i2cd;
+      const double i2z = 0.5 * inv_z;
+
+      for (int j = lane; j < S; j += TS) acc[j] = 0.0;
+      double s00 = 0.0;
+      // (ss|ss) needs no VRR: its only target is the image sum of (00|00)
+      const bool need_vrr = !(pl->want00 && pl->ntg == 1);
+      team_sync<TS>(mask);
+
+      for (int n0 = 0; n0 < ctx.Ng; n0 += TS) {
+         const int n3 = n0 + lane;
+         bool surv = false;
+         double *myfm = fmx + lane * (L + 1);
+         if (n3 < ctx.Ng) {
+            const double g0 = __ldg(ctx.neighs + n3 * 3 + 0), g1 = __ldg(ctx.neighs + n3 * 3 + 1),
+                         g2 = __ldg(ctx.neighs + n3 * 3 + 2);
+            double PQ0 = P[0] - Q[0] - g0, PQ1 = P[1] - Q[1] - g1, PQ2 = P[2] - Q[2] - g2;
+            double rpq2 = (PQ0 * PQ0 + PQ1 * PQ1 + PQ2 * PQ2);
+            double T = rho * rpq2;
+            fm_eval(ctx, L, R, T, Kfac, myfm);
+            s00 += myfm[0];
+            surv = need_vrr && (myfm[0] > 1.e-12);
+         }
+         unsigned bal = (TS > 1) ? ((__ballot_sync(mask, surv) & mask) >> wl) : (surv ? 1u : 0u);
+         while (bal) {
+            const int src = __ffs(bal) - 1;
+            bal &= bal - 1;
+            if (lane == src) {
+               const int n3s = n0 + src;
+               const double g0 = __ldg(ctx.neighs + n3s * 3 + 0), g1 = __ldg(ctx.neighs + n3s * 3 + 1),
+                            g2 = __ldg(ctx.neighs + n3s * 3 + 2);
+               const double Qp0 = Q[0] + g0, Qp1 = Q[1] + g1, Qp2 = Q[2] + g2;
+               const double W0 = (zab * P[0] + zcd * Qp0) * inv_z;
+               const double W1 = (zab * P[1] + zcd * Qp1) * inv_z;
+               const double W2 = (zab * P[2] + zcd * Qp2) * inv_z;
+               pqz[0] = P[0] - A[0]; pqz[1] = P[1] - A[1]; pqz[2] = P[2] - A[2];
+               pqz[3] = W0 - P[0]; pqz[4] = W1 - P[1]; pqz[5] = W2 - P[2];
+               pqz[6] = Q[0] - Cs[0]; pqz[7] = Q[1] - Cs[1]; pqz[8] = Q[2] - Cs[2];
+               pqz[9] = W0 - Qp0; pqz[10] = W1 - Qp1; pqz[11] = W2 - Qp2;
+               pqz[12] = i2ab; pqz[13] = mrab; pqz[14] = i2cd; pqz[15] = mrcd; pqz[16] = i2z;
+               const int n00 = pl->vb[0].nm;
+               for (int q = 0; q < n00; q++) ws[q] = myfm[q];
+            }
+            team_sync<TS>(mask);
+            for (int lv = 1; lv <= pl->nlev; lv++) {
+               const int b0 = pl->lev_off[lv - 1], b1 = pl->lev_off[lv];
+               int tot = 0;
+               for (int bb = b0; bb < b1; bb++) tot += pl->vb[bb].nelem;
+               for (int e = lane; e < tot; e += TS) {
+                  int bb = b0, ee = e;
+                  while (ee >= pl->vb[bb].nelem) { ee -= pl->vb[bb].nelem; bb++; }
+                  vrr_elem(pl->vb[bb], ee, ws, pqz);
+               }
+               team_sync<TS>(mask);
+            }
+            for (int t = 0; t < pl->ntg; t++) {
+               if (pl->want00 && pl->tg_e[t] == 0 && pl->tg_f[t] == 0) continue;
+               const double *srcp = ws + pl->tg_voff[t];
+               double *dst = acc + pl->tg_soff[t];
+               for (int q = lane; q < pl->tg_n[t]; q += TS) dst[q] += srcp[q];
+            }
+            team_sync<TS>(mask);
+         }
+      }
+      if (pl->want00) {
+         if (TS > 1) {
+#pragma unroll
+            for (int o = TS / 2; o > 0; o >>= 1) s00 += __shfl_down_sync(mask, s00, o, TS);
+         }
+         if (lane == 0) acc[pl->s00] += s00;
+      }
+      team_sync<TS>(mask);
+      double *out = bt.AC + (size_t)p * S;
+      for (int j = lane; j < S; j += TS) out[j] = acc[j];
+      team_sync<TS>(mask);
+   }
+}
+
+// ---------------------------------------------------------------------------------------
+// k_group: contraction + HRR + sum over image pairs + spherical transform + K update
+// ---------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_group(DevCtx ctx, BatchArgs bt, int warp_doubles, int use_global) {
+   extern __shared__ __align__(16) double smem[];
+   ClassPlan *pl = reinterpret_cast<ClassPlan *>(smem);
+   {
+      const int nwords = (int)(sizeof(ClassPlan) / 4);
+      const int *src = reinterpret_cast<const int *>(bt.plan);
+      int *dst = reinterpret_cast<int *>(smem);
+      for (int w = threadIdx.x; w < nwords; w += blockDim.x) dst[w] = src[w];
+   }
+   __syncthreads();
+   const int plan_doubles = (int)((sizeof(ClassPlan) + 15) / 16) * 2;
+   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32, nwarp = blockDim.x / 32;
+   const int gwarp = blockIdx.x * nwarp + warp;
+   double *wbase = use_global ? (bt.gscratch + (size_t)gwarp * warp_doubles)
+                              : (smem + plan_doubles + (size_t)warp * warp_doubles);
+   const int S = pl->S, Nc = pl->Nc, Ns = pl->Ns;
+   const int Hws = max(pl->H, 2 * Nc);
+   double *ws = wbase;           // HRR workspace (contracted targets first) [Hws]
+   double *cart = wbase + Hws;   // sum over shells [Nc]
+   const int la = pl->la, lb = pl->lb, lc = pl->lc, ld = pl->ld;
+   const int nca = ncart(la), ncb = ncart(lb), ncc = ncart(lc), ncd_ = ncart(ld);
+   const int nsa = 2 * la + 1, nsb = 2 * lb + 1, nsc = 2 * lc + 1, nsd = 2 * ld + 1;
+
+   for (uint32_t g = gwarp; g < bt.ngroup; g += gridDim.x * nwarp) {
+      const GroupRec G = bt.groups[g];
+      const int nl1 = G.nl[1], nl2 = G.nl[2], nl3 = G.nl[3];
+      const int nlabcd = G.nl[0] * nl1 * nl2 * nl3;
+      for (int r = 0; r < nlabcd; r++) {
+         const int ia = r / (nl1 * nl2 * nl3), ib = (r / (nl2 * nl3)) % nl1, ic = (r / nl3) % nl2, id = r % nl3;
+         for (int q = lane; q < Nc; q += 32) cart[q] = 0.0;
+         for (uint32_t s = 0; s < G.nshell; s++) {
+            const ShellRec sh = bt.shells[G.shell_off + s];
+            const BasisEnt ea = ctx.ents[sh.ent[0]], eb = ctx.ents[sh.ent[1]];
+            const BasisEnt ec = ctx.ents[sh.ent[2]], ed = ctx.ents[sh.ent[3]];
+            const double *Ka = ctx.pool + ea.k_off + ia * ea.np;
+            const double *Kb = ctx.pool + eb.k_off + ib * eb.np;
+            const double *Kc = ctx.pool + ec.k_off + ic * ec.np;
+            const double *Kd = ctx.pool + ed.k_off + id * ed.np;
+            // contraction over primitives (reference src/compute_ECO.cpp:131-212)
+            for (int j = lane; j < S; j += 32) {
+               double a = 0.0;
+               for (uint32_t ip = 0; ip < sh.nprm; ip++) {
+                  const uint32_t code = bt.prm[sh.prm_off + ip];
+                  const double kp = __ldg(Ka + (code >> 24)) * __ldg(Kb + ((code >> 16) & 255)) *
+                                    __ldg(Kc + ((code >> 8) & 255)) * __ldg(Kd + (code & 255));
+                  a += kp * bt.AC[(size_t)(sh.prm_off + ip) * S + j];
+               }
+               ws[j] = a;
+            }
+            __syncwarp();
+            double A[3], B[3], C[3], D[3], CDs[3];
+            shell_geom(ctx, ea, eb, ec, ed, sh.n1, sh.n2, A, B, C, D, CDs);
+            const double AB[3] = {A[0] - B[0], A[1] - B[1], A[2] - B[2]};
+            const double CD[3] = {C[0] - D[0], C[1] - D[1], C[2] - D[2]};
+            // HRR (reference src/compute_HRR.cpp:7-99)
+            for (int lv = 1; lv <= pl->nhlev; lv++) {
+               for (int o = pl->hlev_off[lv - 1]; o < pl->hlev_off[lv]; o++) {
+                  const HOp h = pl->hop[o];
+                  if (h.type == 0) {
+                     const int c = h.x, d = h.y;
+                     const int nc_ = ncart(c), nd = ncart(d), ncp = ncart(c + 1), ndm = ncart(d - 1);
+                     for (int e = lane; e < h.nelem; e += 32) {
+                        const int l = e % nd, k = (e / nd) % nc_, ie = e / (nd * nc_);
+                        const int dir = c_cart_dir[d][l];
+                        const int lm = c_cart_dec[d][l][dir];
+                        const int kp = c_cart_inc[c][k][dir];
+                        ws[h.out + e] = ws[h.in1 + (ie * ncp + kp) * ndm + lm] + CD[dir] * ws[h.in2 + (ie * nc_ + k) * ndm + lm];
+                     }
+                  } else {
+                     const int a = h.x, b = h.y;
+                     const int nb = ncart(b), nbm = ncart(b - 1), cdn = ncc * ncd_;
+                     for (int e = lane; e < h.nelem; e += 32) {
+                        const int q = e % cdn, j = (e / cdn) % nb, i = e / (cdn * nb);
+                        const int dir = c_cart_dir[b][j];
+                        const int jm = c_cart_dec[b][j][dir];
+                        const int ip = c_cart_inc[a][i][dir];
+                        ws[h.out + e] = ws[h.in1 + (ip * nbm + jm) * cdn + q] + AB[dir] * ws[h.in2 + (i * nbm + jm) * cdn + q];
+                     }
+                  }
+               }
+               __syncwarp();
+            }
+            for (int q = lane; q < Nc; q += 32) cart[q] += ws[pl->out_off + q];
+            __syncwarp();
+         }
+         // cartesian -> spherical, one centre at a time (a, b, c, d)
+         {
+            int dims[4] = {nca, ncb, ncc, ncd_};
+            const int ls[4] = {la, lb, lc, ld};
+            const int ns[4] = {nsa, nsb, nsc, nsd};
+            const double *src = cart;
+            for (int ctr = 0; ctr < 4; ctr++) {
+               double *dst = ws + ((ctr & 1) ? Nc : 0);
+               int od[4] = {dims[0], dims[1], dims[2], dims[3]};
+               od[ctr] = ns[ctr];
+               const int tot = od[0] * od[1] * od[2] * od[3];
+               const int nk = dims[ctr];
+               const double *cc = c_c2s[ls[ctr]];
+               int stride = 1;
+               for (int q = ctr + 1; q < 4; q++) stride *= dims[q];
+               for (int t = lane; t < tot; t += 32) {
+                  int rem = t, id4[4];
+                  for (int q = 3; q >= 0; q--) { id4[q] = rem % od[q]; rem /= od[q]; }
+                  const int mi = id4[ctr];
+                  id4[ctr] = 0;
+                  const int base = ((id4[0] * dims[1] + id4[1]) * dims[2] + id4[2]) * dims[3] + id4[3];
+                  double acc = 0.0;
+                  for (int k = 0; k < nk; k++) acc += cc[mi * nk + k] * src[base + k * stride];
+                  dst[t] = acc;
+               }
+               __syncwarp();
+               dims[ctr] = ns[ctr];
+               src = dst;
+            }
+         }
+         const double *sph = ws + Nc;   // after 4 passes the result sits in the odd buffer
+         // K update (reference src/compute_KS.cpp:26-115)
+         const QrttRec k = bt.qrtts[G.qrtt_off + r];
+         const double fac = c_symm[k.idx_fac] * ctx.hf_fac;
+         const int nscd = nsc * nsd, nsbcd = nsb * nscd;
+         for (int t = lane; t < Ns; t += 32) {
+            const int isa = t / nsbcd, isb = (t / nscd) % nsb, isc = (t / nsd) % nsc, isd = t % nsd;
+            const int iac = !(k.T & 1) ? isc * k.ld[0] + isa : isa * k.ld[0] + isc;
+            const int iad = !(k.T & 2) ? isd * k.ld[1] + isa : isa * k.ld[1] + isd;
+            const int ibc = !(k.T & 4) ? isc * k.ld[2] + isb : isb * k.ld[2] + isc;
+            const int ibd = !(k.T & 8) ? isd * k.ld[3] + isb : isb * k.ld[3] + isd;
+            const size_t Iac = (size_t)k.off[0] + iac, Iad = (size_t)k.off[1] + iad;
+            const size_t Ibc = (size_t)k.off[2] + ibc, Ibd = (size_t)k.off[3] + ibd;
+            if (Iac >= ctx.FP_size || Iad >= ctx.FP_size || Ibc >= ctx.FP_size || Ibd >= ctx.FP_size) {
+               atomicOr(ctx.err, 1);
+               continue;
+            }
+            const double iabcd = -fac * sph[t];
+            for (int sp = 0; sp < ctx.nspin; sp++) {
+               const double *Pm = ctx.P[sp];
+               double *Km = ctx.K[sp];
+               atomicAdd(Km + Ibd, iabcd * __ldg(Pm + Iac));
+               atomicAdd(Km + Ibc, iabcd * __ldg(Pm + Iad));
+               atomicAdd(Km + Iad, iabcd * __ldg(Pm + Ibc));
+               atomicAdd(Km + Iac, iabcd * __ldg(Pm + Ibd));
+            }
+         }
+         __syncwarp();
+      }
+   }
+}
+
+// ---------------------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------------------
+static int h_ncart(int l) { return (l + 1) * (l + 2) / 2; }
+static int h_cidx(int x, int y, int z) { int a = y + z; return a * (a + 1) / 2 + z; }
+
+cudaError_t upload_constant_tables(const double *c2s_l0to3, const double *symm5) {
+   int8_t exp_[8][36][3] = {}, dir[8][36] = {}, dec[8][36][3], inc[8][36][3];
+   for (int l = 0; l < 8; l++) for (int i = 0; i < 36; i++) for (int q = 0; q < 3; q++) { dec[l][i][q] = -1; inc[l][i][q] = -1; }
+   for (int l = 0; l < 8; l++) {
+      for (int i = 0; i < h_ncart(l); i++) {
+         int a = 0; while ((a + 1) * (a + 2) / 2 <= i) a++;
+         int e[3]; e[0] = l - a; e[2] = i - a * (a + 1) / 2; e[1] = a - e[2];
+         for (int q = 0; q < 3; q++) exp_[l][i][q] = (int8_t)e[q];
+         dir[l][i] = (int8_t)(e[0] ? 0 : (e[1] ? 1 : 2));
+         for (int q = 0; q < 3; q++) {
+            int f[3] = {e[0], e[1], e[2]};
+            if (f[q] > 0) { f[q]--; dec[l][i][q] = (int8_t)h_cidx(f[0], f[1], f[2]); }
+            int g[3] = {e[0], e[1], e[2]};
+            g[q]++;
+            if (l + 1 < 8) inc[l][i][q] = (int8_t)h_cidx(g[0], g[1], g[2]);
+         }
+      }
+   }
+   cudaError_t err;
+   if ((err = cudaMemcpyToSymbol(c_cart_exp, exp_, sizeof(exp_))) != cudaSuccess) return err;
+   if ((err = cudaMemcpyToSymbol(c_cart_dir, dir, sizeof(dir))) != cudaSuccess) return err;
+   if ((err = cudaMemcpyToSymbol(c_cart_dec, dec, sizeof(dec))) != cudaSuccess) return err;
+   if ((err = cudaMemcpyToSymbol(c_cart_inc, inc, sizeof(inc))) != cudaSuccess) return err;
+   if ((err = cudaMemcpyToSymbol(c_c2s, c2s_l0to3, sizeof(double) * 4 * 70)) != cudaSuccess) return err;
+   return cudaMemcpyToSymbol(c_symm, symm5, sizeof(double) * 5);
+}
+
+int plan_smem_doubles() { return (int)((sizeof(ClassPlan) + 15) / 16) * 2; }
+
+static int g_max_smem = 0;
+static int max_dyn_smem() {
+   if (!g_max_smem) {
+      int dev = 0; cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&g_max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+      if (g_max_smem <= 0) g_max_smem = 48 * 1024;
+   }
+   return g_max_smem;
+}
+
+template <int TS>
+static cudaError_t launch_prim_t(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan &hp, cudaStream_t st) {
+   const int L = hp.L;
+   int team_doubles = hp.V + hp.S + 17 + TS * (L + 1);
+   team_doubles = (team_doubles + 1) & ~1;
+   const int budget = std::min(max_dyn_smem(), 200 * 1024);
+   const size_t plan_bytes = (size_t)plan_smem_doubles() * 8;
+   int teams = (int)((budget - (int)plan_bytes) / ((size_t)team_doubles * 8));
+   teams = std::min(teams, 256 / TS);
+   if (teams < 1) return cudaErrorInvalidConfiguration;
+   const size_t smem = plan_bytes + (size_t)teams * team_doubles * 8;
+   cudaFuncSetAttribute(k_prim<TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+   long blocks = ((long)bt.nprm + teams - 1) / teams;
+   blocks = std::max(1L, std::min(blocks, 148L * 64));
+   k_prim<TS><<<(unsigned)blocks, teams * TS, smem, st>>>(ctx, bt, team_doubles);
+   return cudaGetLastError();
+}
+
+int prim_team_size(const ClassPlan &hp) {
+   const int w = hp.V + hp.S;
+   if (w <= 40) return 1;
+   if (w <= 300) return 4;
+   if (w <= 1200) return 8;
+   return 32;
+}
+
+cudaError_t launch_prim(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan &hp, cudaStream_t st) {
+   if (bt.nprm == 0) return cudaSuccess;
+   switch (prim_team_size(hp)) {
+      case 1: return launch_prim_t<1>(ctx, bt, hp, st);
+      case 4: return launch_prim_t<4>(ctx, bt, hp, st);
+      case 8: return launch_prim_t<8>(ctx, bt, hp, st);
+      default: return launch_prim_t<32>(ctx, bt, hp, st);
+   }
+}
+
+size_t group_warp_doubles(const ClassPlan &hp) {
+   size_t d = (size_t)std::max(hp.H, 2 * hp.Nc) + hp.Nc;
+   return (d + 1) & ~(size_t)1;
+}
+
+// returns the number of global-scratch doubles needed (0 if the shared-memory path is used)
+size_t group_global_scratch(const ClassPlan &hp, int *grid, int *warps) {
+   const size_t wd = group_warp_doubles(hp);
+   const int budget = std::min(max_dyn_smem(), 200 * 1024) - plan_smem_doubles() * 8;
+   int nw = (int)(budget / (wd * 8));
+   if (nw >= 1) return 0;
+   *warps = 4;
+   *grid = 148 * 2;
+   return wd * (size_t)(*warps) * (*grid);
+}
+
+cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan &hp, cudaStream_t st) {
+   if (bt.ngroup == 0) return cudaSuccess;
+   const size_t wd = group_warp_doubles(hp);
+   const size_t plan_bytes = (size_t)plan_smem_doubles() * 8;
+   const int budget = std::min(max_dyn_smem(), 200 * 1024);
+   int nw = (int)((budget - (int)plan_bytes) / (wd * 8));
+   if (nw >= 1) {
+      nw = std::min(nw, 8);
+      const size_t smem = plan_bytes + (size_t)nw * wd * 8;
+      cudaFuncSetAttribute(k_group, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      long blocks = ((long)bt.ngroup + nw - 1) / nw;
+      blocks = std::max(1L, std::min(blocks, 148L * 64));
+      k_group<<<(unsigned)blocks, nw * 32, smem, st>>>(ctx, bt, (int)wd, 0);
+   } else {
+      int grid = 0, warps = 0;
+      group_global_scratch(hp, &grid, &warps);
+      cudaFuncSetAttribute(k_group, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan_bytes);
+      k_group<<<grid, warps * 32, plan_bytes, st>>>(ctx, bt, (int)wd, 1);
+   }
+   return cudaGetLastError();
+}
+
+}  // namespace gint

@@ -1,0 +1,51 @@
+// kernels.h -- device context, batch arguments and launchers of the K-build kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+#include "engine_types.h"
+
+namespace gint {
+
+// Everything the kernels read besides the batch records (device pointers).
+struct DevCtx {
+   const double *pool;        // exponents and normalised coefficients
+   const BasisEnt *ents;
+   const double *neighs;      // Ng lattice vectors
+   int Ng;
+   int nspin;
+   double cell[18];           // h (rows = lattice vectors) and h^-1
+   double R_cut;
+   const double *C0;
+   int ld_C0;
+   const uint8_t *lut_low, *lut_high;   // 128 x 128 patch maps
+   const double *bw;          // per patch: B1, W1, B2, W2
+   const double *ftable;      // Boys table, 121 x 28
+   const double *P[2];
+   double *K[2];
+   double hf_fac;
+   size_t FP_size;
+   int *err;
+};
+
+// One class-sorted segment of a batch (device pointers).
+struct BatchArgs {
+   const ClassPlan *plan;
+   const uint32_t *prm;       // primitive quartet codes (ipa<<24|ipb<<16|ipc<<8|ipd)
+   const uint32_t *prm_shell; // shell of each primitive quartet
+   const ShellRec *shells;
+   const GroupRec *groups;
+   const QrttRec *qrtts;
+   uint32_t nprm, nshell, ngroup;
+   double *AC;                // [nprm][S] image-summed VRR targets
+   double *gscratch;          // HRR workspace in global memory for the largest classes
+};
+
+bool build_class_plan(int la, int lb, int lc, int ld, ClassPlan &p);
+cudaError_t upload_constant_tables(const double *c2s_l0to3, const double *symm5);
+cudaError_t launch_prim(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan &hp, cudaStream_t st);
+cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan &hp, cudaStream_t st);
+size_t group_global_scratch(const ClassPlan &hp, int *grid, int *warps);
+int prim_team_size(const ClassPlan &hp);
+
+}  // namespace gint

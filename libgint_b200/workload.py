@@ -1,0 +1,187 @@
+"""Synthetic water workloads and the C-ABI replayer (ctypes front end of libgint_driver.so).
+
+The driver library plays the caller of the libGint C-ABI: it generates seeded water systems,
+screens the set/primitive quartets, and replays the add_* stream through any library exporting
+the libgint_* entry points. The named configurations follow the benchmark definitions:
+
+  small_l2      4 water-like molecules, 12 A box, no PBC, l<=2 basis, 20 occupied orbitals
+  periodic_l2   32 molecules, 9.86 A cubic cell, 27 images, l<=2, 128 occupied orbitals
+  periodic_l3   64 molecules, 12.4 A cell, 125 images, l<=3 basis with general contraction
+"""
+import ctypes
+import os
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBDIR = os.path.join(_HERE, "lib")
+DRIVER_SO = os.path.join(LIBDIR, "libgint_driver.so")
+ENGINE_SO = os.path.join(LIBDIR, "libgint_b200.so")
+
+
+class GdConfig(ctypes.Structure):
+    _fields_ = [("n_mol", ctypes.c_int), ("box_ang", ctypes.c_double), ("periodic", ctypes.c_int),
+                ("n_img_1d", ctypes.c_int), ("basis", ctypes.c_int), ("n_occ", ctypes.c_int),
+                ("rc_ang", ctypes.c_double), ("eps_schwarz", ctypes.c_double),
+                ("seed", ctypes.c_uint64), ("full_enum", ctypes.c_int), ("max_prm", ctypes.c_int),
+                ("max_ncontr", ctypes.c_int)]
+
+
+class GdInfo(ctypes.Structure):
+    _fields_ = [("n_bf", ctypes.c_int), ("n_sets", ctypes.c_int), ("n_atoms", ctypes.c_int),
+                ("Ng", ctypes.c_int), ("n_setq", ctypes.c_long), ("n_shells", ctypes.c_long),
+                ("n_prims", ctypes.c_long), ("n_qrtt", ctypes.c_long), ("rc_bohr", ctypes.c_double),
+                ("nder", ctypes.c_int), ("ld_C0", ctypes.c_int), ("C0_size", ctypes.c_int),
+                ("max_abs_P", ctypes.c_double), ("flat_size", ctypes.c_long)]
+
+
+CONFIGS = {
+    "small_l2": dict(n_mol=4, box_ang=12.0, periodic=0, n_img_1d=1, basis=2, n_occ=20),
+    "periodic_l2": dict(n_mol=32, box_ang=9.86, periodic=1, n_img_1d=3, basis=2, n_occ=128),
+    "periodic_l3": dict(n_mol=64, box_ang=12.4, periodic=1, n_img_1d=5, basis=3, n_occ=256),
+}
+
+_D = ctypes.POINTER(ctypes.c_double)
+_lib = None
+
+
+def driver():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(DRIVER_SO):
+            raise RuntimeError(f"{DRIVER_SO} is missing: run libgint_b200.build.build_all()")
+        lib = ctypes.CDLL(DRIVER_SO)
+        lib.gd_create.restype = ctypes.c_void_p
+        lib.gd_create.argtypes = [ctypes.POINTER(GdConfig)]
+        lib.gd_free.argtypes = [ctypes.c_void_p]
+        lib.gd_get_info.argtypes = [ctypes.c_void_p, ctypes.POINTER(GdInfo)]
+        lib.gd_get_P.argtypes = [ctypes.c_void_p, _D]
+        lib.gd_get_C0.argtypes = [ctypes.c_void_p, _D]
+        lib.gd_get_Pflat.argtypes = [ctypes.c_void_p, _D]
+        lib.gd_unpack_K.argtypes = [ctypes.c_void_p, _D, _D]
+        lib.gd_get_sets.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
+        lib.gd_get_setq.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_long)]
+        lib.gd_api_open.restype = ctypes.c_void_p
+        lib.gd_api_open.argtypes = [ctypes.c_char_p]
+        lib.gd_api_symbol.restype = ctypes.c_void_p
+        lib.gd_api_symbol.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+        lib.gd_setup.restype = ctypes.c_void_p
+        lib.gd_setup.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+        lib.gd_build_K.restype = ctypes.c_double
+        lib.gd_build_K.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _D, _D,
+                                   ctypes.c_long, ctypes.c_long, _D]
+        lib.gd_teardown.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        lib.gd_tcg_table.restype = ctypes.c_int
+        lib.gd_tcg_table.argtypes = [ctypes.c_int, _D]
+        lib.gd_tcg_exact.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, _D]
+        lib.gd_boys.argtypes = [ctypes.c_int, ctypes.c_double, _D]
+        _lib = lib
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(_D)
+
+
+class Workload:
+    """A generated system plus its screened add_* call stream."""
+
+    def __init__(self, name=None, seed=0, eps_schwarz=1e-11, rc_ang=6.0, full_enum=False,
+                 max_prm=16, max_ncontr=4, **overrides):
+        params = dict(CONFIGS[name]) if name else {}
+        params.update(overrides)
+        cfg = GdConfig(n_mol=params["n_mol"], box_ang=params["box_ang"],
+                       periodic=params["periodic"], n_img_1d=params["n_img_1d"],
+                       basis=params["basis"], n_occ=params["n_occ"], rc_ang=rc_ang,
+                       eps_schwarz=eps_schwarz, seed=seed, full_enum=int(full_enum),
+                       max_prm=max_prm, max_ncontr=max_ncontr)
+        self.name = name
+        self.params = params
+        self._w = driver().gd_create(ctypes.byref(cfg))
+        inf = GdInfo()
+        driver().gd_get_info(self._w, ctypes.byref(inf))
+        self.info = {f: getattr(inf, f) for f, _ in GdInfo._fields_}
+        self.n_bf = inf.n_bf
+
+    def __del__(self):
+        if getattr(self, "_w", None) and _lib is not None:
+            _lib.gd_free(self._w)
+            self._w = None
+
+    @property
+    def P(self):
+        P = np.empty(self.n_bf * self.n_bf)
+        driver().gd_get_P(self._w, _dp(P))
+        return P
+
+    @property
+    def Pflat(self):
+        """P in the packed set-pair block layout (what set_P receives)."""
+        P = np.empty(self.info["flat_size"])
+        driver().gd_get_Pflat(self._w, _dp(P))
+        return P
+
+    def unpack_K(self, K_flat):
+        """Dense symmetric exchange matrix from the packed K returned by get_K."""
+        K = np.empty(self.n_bf * self.n_bf)
+        driver().gd_unpack_K(self._w, _dp(np.ascontiguousarray(K_flat)), _dp(K))
+        return K.reshape(self.n_bf, self.n_bf)
+
+    def exchange_energy(self, K_flat):
+        """E_x = 1/4 sum P K (closed shell, P = 2 C C^T, hf_fac = 1)."""
+        n = self.n_bf
+        return 0.25 * float(np.sum(self.P.reshape(n, n) * self.unpack_K(K_flat)))
+
+    @property
+    def C0(self):
+        C0 = np.empty(self.info["C0_size"])
+        driver().gd_get_C0(self._w, _dp(C0))
+        return C0
+
+    def sets(self):
+        out = np.empty((self.info["n_sets"], 4), dtype=np.int32)
+        driver().gd_get_sets(self._w, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+        return out
+
+    def setq(self):
+        out = np.empty((self.info["n_setq"], 6), dtype=np.int64)
+        driver().gd_get_setq(self._w, out.ctypes.data_as(ctypes.POINTER(ctypes.c_long)))
+        return out
+
+
+class Api:
+    """One loaded library that exports the libgint_* C-ABI."""
+
+    def __init__(self, so_path):
+        self.path = so_path
+        self._a = driver().gd_api_open(so_path.encode())
+        if not self._a:
+            raise RuntimeError(f"cannot load the libgint C-ABI from {so_path}")
+
+    def symbol(self, name, restype=None, argtypes=None):
+        addr = driver().gd_api_symbol(self._a, name.encode())
+        if not addr:
+            return None
+        return ctypes.CFUNCTYPE(restype, *(argtypes or []))(addr)
+
+
+class Session:
+    """A handle of one library set up for one workload (everything before set_P)."""
+
+    def __init__(self, api, wl, max_mem_mb=7000):
+        self.api, self.wl = api, wl
+        self.h = driver().gd_setup(wl._w, api._a, max_mem_mb)
+
+    def build_K(self, P=None, q0=0, q1=-1):
+        """One K build (set_P, add_* stream, get_K). Returns (K_flat, wall_ms, [setP, stream, getK] ms)."""
+        K = np.zeros(self.wl.info["flat_size"])
+        t = np.zeros(3)
+        Pp = None if P is None else _dp(np.ascontiguousarray(P, dtype=np.float64))
+        ms = driver().gd_build_K(self.wl._w, self.api._a, self.h, Pp, _dp(K), q0, q1, _dp(t))
+        return K, ms, t
+
+    def close(self):
+        if self.h:
+            driver().gd_teardown(self.api._a, self.h)
+            self.h = None
+
+
