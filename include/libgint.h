@@ -18,7 +18,8 @@
  * Differences from the reference, all additive:
  *   - errors never terminate the process; they are recorded and read with libgint_last_error;
  *   - libgint_destroy_handle releases a handle;
- *   - libgint_set_precision / libgint_get_stats / libgint_rebuild_K are extensions.
+ *   - record/replay of the device-resident quartet list, counters and statistics are
+ *     extensions declared at the end of this header.
  * Threading: one handle per host thread; handles are independent (each owns its stream and
  * device buffers), so the reference's team-collective calls need no omp barrier here.
  */
@@ -96,6 +97,29 @@ void libgint_destroy_handle(void *handle);
  * targets, HRR workspace (doubles), cartesian and spherical block sizes, VRR blocks, HRR
  * steps, primitive team size; returns 0 for an unsupported class */
 int libgint_plan_sizes(int la, int lb, int lc, int ld, int *out);
+/* on = 1: keep the device batches of the following K build(s) (the screened quartet list of
+ * an SCF step); on = 0: stop recording */
+void libgint_record(void *handle, int on);
+/* recompute K from the recorded quartet list with the current P (after libgint_set_P), without
+ * the add_* stream; K is then read with libgint_get_K. Returns the device time in ms. */
+double libgint_replay(void *handle);
+/* libgint_replay with the summed device time per kernel kind: kt[0] = Fm+VRR kernel,
+ * kt[1] = contraction+HRR+spherical+K kernel (ms) */
+double libgint_replay_profile(void *handle, double *kt);
+/* algorithmic FP64 operation counts of class (la,lb,lc,ld) following the reference recursion:
+ * out[0] per Chebyshev G_m evaluation, [1] per Boys evaluation, [2] VRR per image, [3] image
+ * sum per image, [4] contraction per primitive and row, [5] HRR per shell and row,
+ * [6] spherical transform per row, [7] K update per row */
+int libgint_plan_flops(int la, int lb, int lc, int ld, double *out);
+/* per-class device event counters: out[c*4 + {0,1,2,3}] = Chebyshev G_m evaluations, Boys
+ * evaluations, images through the VRR, primitive quartets; c = la*64 + lb*16 + lc*4 + ld */
+void libgint_set_counters(void *handle, int on);
+void libgint_get_counters(void *handle, unsigned long long *out);
+/* out[0..5] = shell quartets, primitive quartets, groups, batches, kernel launches, bytes
+ * copied host -> device */
+void libgint_get_stats(void *handle, long long *out);
+/* FP64 FMA rate of the current GPU (TFLOP/s), measured by a dependent-FMA kernel */
+double libgint_fp64_peak_tflops(void);
 
 #ifdef __cplusplus
 }

@@ -43,6 +43,15 @@ SIGNATURES = {
     "libgint_last_error": (ctypes.c_int, [_V]),
     "libgint_error_string": (ctypes.c_char_p, [_V]),
     "libgint_destroy_handle": (None, [_V]),
+    "libgint_plan_sizes": (ctypes.c_int, [ctypes.c_int] * 4 + [_I]),
+    "libgint_record": (None, [_V, ctypes.c_int]),
+    "libgint_replay": (ctypes.c_double, [_V]),
+    "libgint_replay_profile": (ctypes.c_double, [_V, _D]),
+    "libgint_plan_flops": (ctypes.c_int, [ctypes.c_int] * 4 + [_D]),
+    "libgint_set_counters": (None, [_V, ctypes.c_int]),
+    "libgint_get_counters": (None, [_V, ctypes.POINTER(ctypes.c_ulonglong)]),
+    "libgint_get_stats": (None, [_V, ctypes.POINTER(ctypes.c_longlong)]),
+    "libgint_fp64_peak_tflops": (ctypes.c_double, []),
 }
 
 

@@ -604,6 +604,15 @@ void gd_get_sets(const gd_workload *w, int *out) {
    }
 }
 
+// normalised coefficients of set s (nl*np) and its exponents; returns np
+int gd_get_coeffs(const gd_workload *w, int s, double *K, double *Z, int *nl) {
+   const SetDef &d = w->defs[w->sets[s].def];
+   std::memcpy(K, d.Knorm.data(), sizeof(double) * d.Knorm.size());
+   std::memcpy(Z, d.Z.data(), sizeof(double) * d.Z.size());
+   *nl = d.nl;
+   return d.np;
+}
+
 // per set quartet {i,j,k,l,n_shells,n_prims} (for cost/class statistics)
 void gd_get_setq(const gd_workload *w, long *out) {
    for (size_t q = 0; q < w->setq.size(); q++) {
@@ -690,16 +699,30 @@ void *gd_setup(const gd_workload *w, gd_api *a, int max_mem_mb) {
 
 // One K build: set_P, the add_* stream of set quartets [q0, q1), get_K. Returns wall ms.
 // times[0] = set_P, [1] = stream, [2] = get_K (ms). P == nullptr uses the workload's P.
+static double build_K_impl(const gd_workload *w, gd_api *a, void *h, const double *P, double *K,
+                           long q0, long q1, const long *idx, double *times);
+
 double gd_build_K(const gd_workload *w, gd_api *a, void *h, const double *P, double *K,
                   long q0, long q1, double *times) {
+   return build_K_impl(w, a, h, P, K, q0, q1, nullptr, times);
+}
+
+// the same for an explicit list of set quartets idx[0..n)
+double gd_build_K_subset(const gd_workload *w, gd_api *a, void *h, const double *P, double *K,
+                         const long *idx, long n, double *times) {
+   return build_K_impl(w, a, h, P, K, 0, n, idx, times);
+}
+
+static double build_K_impl(const gd_workload *w, gd_api *a, void *h, const double *P, double *K,
+                           long q0, long q1, const long *idx, double *times) {
    using clk = std::chrono::steady_clock;
    const int S = (int)w->sets.size();
-   if (q1 < 0 || q1 > (long)w->setq.size()) q1 = (long)w->setq.size();
+   if (!idx && (q1 < 0 || q1 > (long)w->setq.size())) q1 = (long)w->setq.size();
    auto t0 = clk::now();
    a->setP(h, const_cast<double *>(P ? P : w->Pflat.data()), (int)w->flat_size);
    auto t1 = clk::now();
-   for (long iq = q0; iq < q1; iq++) {
-      const SetQ &q = w->setq[iq];
+   for (long iq0 = q0; iq0 < q1; iq0++) {
+      const SetQ &q = w->setq[idx ? idx[iq0] : iq0];
       const Set *s4[4] = {&w->sets[q.i], &w->sets[q.j], &w->sets[q.k], &w->sets[q.l]};
       const SetDef *d4[4] = {&w->defs[s4[0]->def], &w->defs[s4[1]->def], &w->defs[s4[2]->def], &w->defs[s4[3]->def]};
       for (uint32_t hs = q.shell_begin; hs < q.shell_end; hs++) {

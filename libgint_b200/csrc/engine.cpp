@@ -100,9 +100,16 @@ struct HostSet {
    bool defined = false;
 };
 
-struct PendShell { int cls; uint32_t ent[4]; uint16_t n1, n2; uint32_t prm_off, nprm; };
-struct PendQrt { int cls; uint8_t nl[4]; };
-struct PendQrtt { int cls; QrttRec rec; };
+// A group being filled by the current set quartet: the records go straight into the class
+// queue and are committed (or rolled back) by add_set.
+struct OpenGroup {
+   int cls;
+   uint32_t shell_off, qrtt_off;
+   size_t prm_off;
+   uint8_t nl[4];
+   bool have_qrt;
+   int nq;
+};
 
 struct ClassQ {
    std::vector<uint32_t> prm, prm_shell;
@@ -155,17 +162,26 @@ struct Handle {
    bool plans_ready = false;
    // streaming state
    std::vector<uint32_t> prm_tmp;
-   std::vector<PendShell> set_shells;
-   std::vector<uint32_t> set_prms;
-   std::vector<PendQrt> set_qrts;
-   std::vector<PendQrtt> set_qrtts;
+   OpenGroup open[64];
+   int nopen = 0;
+   int open_of[256];
    ClassQ q[256];
    std::vector<int> active;
    size_t pend_prims = 0, pend_ac = 0, pend_rec = 0;
    Slot slots[2];
    int cur = 0;
+   // record / replay of the device-resident quartet list
+   struct RecSeg { int c; size_t o_prm, o_ps, o_sh, o_g, o_q, ac_off; uint32_t nprm, nshell, ngroup; };
+   struct RecBatch { DBuf rec; std::vector<RecSeg> segs; size_t ac_doubles = 0; };
+   bool recording = false;
+   std::vector<RecBatch> recs;
+   DBuf rec_ac, rec_gscr;
+   // optional device event counters [256 classes][4]
+   DBuf d_cnt;
+   bool counting = false;
+   long long n_launch = 0;
    // statistics
-   long long n_shells = 0, n_prims = 0, n_groups = 0, n_flush = 0;
+   long long n_shells = 0, n_prims = 0, n_groups = 0, n_flush = 0, h2d_bytes = 0;
 };
 
 static void set_error(Handle *h, int code, const std::string &msg) {
@@ -190,6 +206,24 @@ static bool ensure(Handle *h, DBuf &b, size_t bytes, const char *what) {
 static void release(DBuf &b) { if (b.p) cudaFree(b.p); b.p = nullptr; b.bytes = 0; }
 
 static inline int cls_of(int la, int lb, int lc, int ld) { return la * 64 + lb * 16 + lc * 4 + ld; }
+
+static inline OpenGroup *open_group(Handle *h, int c) {
+   int o = h->open_of[c];
+   if (o >= 0) return &h->open[o];
+   if (h->nopen >= 64) return nullptr;
+   o = h->nopen++;
+   h->open_of[c] = o;
+   OpenGroup &g = h->open[o];
+   ClassQ &Q = h->q[c];
+   g.cls = c;
+   g.shell_off = (uint32_t)Q.shells.size();
+   g.qrtt_off = (uint32_t)Q.qrtts.size();
+   g.prm_off = Q.prm.size();
+   g.nl[0] = g.nl[1] = g.nl[2] = g.nl[3] = 0;
+   g.have_qrt = false;
+   g.nq = 0;
+   return &g;
+}
 
 static void ensure_ent_base(Handle *h);
 
@@ -307,6 +341,7 @@ static DevCtx make_ctx(Handle *h) {
    c.hf_fac = h->hf_fac;
    c.FP_size = h->FP_size;
    c.err = (int *)h->d_err.p;
+   c.cnt = h->counting ? (unsigned long long *)h->d_cnt.p : nullptr;
    return c;
 }
 
@@ -370,14 +405,25 @@ static void flush(Handle *h) {
       std::memcpy(s.h_stage + g.o_g, Q.groups.data(), Q.groups.size() * sizeof(GroupRec));
       std::memcpy(s.h_stage + g.o_q, Q.qrtts.data(), Q.qrtts.size() * sizeof(QrttRec));
    }
-   if (!ck(h, cudaMemcpyAsync(s.rec.p, s.h_stage, off, cudaMemcpyHostToDevice, h->stream), "record upload")) return;
+   char *dev_rec = (char *)s.rec.p;
+   Handle::RecBatch *rb = nullptr;
+   if (h->recording) {
+      h->recs.emplace_back();
+      rb = &h->recs.back();
+      if (!ensure(h, rb->rec, off, "recorded batch")) return;
+      dev_rec = (char *)rb->rec.p;
+      rb->ac_doubles = ac;
+   }
+   if (!ck(h, cudaMemcpyAsync(dev_rec, s.h_stage, off, cudaMemcpyHostToDevice, h->stream), "record upload")) return;
+   h->h2d_bytes += (long long)off;
    DevCtx ctx = make_ctx(h);
    for (const Seg &g : segs) {
       ClassQ &Q = h->q[g.c];
       const ClassPlan &hp = h->plans[g.c];
       BatchArgs bt;
       std::memset(&bt, 0, sizeof(bt));
-      char *base = (char *)s.rec.p;
+      char *base = dev_rec;
+      bt.cls = g.c;
       bt.plan = (const ClassPlan *)h->d_plans.p + g.c;
       bt.prm = (const uint32_t *)(base + g.o_prm);
       bt.prm_shell = (const uint32_t *)(base + g.o_ps);
@@ -396,6 +442,8 @@ static void flush(Handle *h) {
       }
       if (!ck(h, launch_prim(ctx, bt, hp, h->stream), "k_prim launch")) return;
       if (!ck(h, launch_group(ctx, bt, hp, h->stream), "k_group launch")) return;
+      h->n_launch += 2;
+      if (rb) rb->segs.push_back({g.c, g.o_prm, g.o_ps, g.o_sh, g.o_g, g.o_q, g.ac_off, bt.nprm, bt.nshell, bt.ngroup});
       h->n_prims += bt.nprm; h->n_shells += bt.nshell; h->n_groups += bt.ngroup;
       Q.prm.clear(); Q.prm_shell.clear(); Q.shells.clear(); Q.groups.clear(); Q.qrtts.clear();
       Q.active = false;
@@ -428,6 +476,7 @@ static void set_P_impl(Handle *h, int nspin, const double *Pa, const double *Pb,
    for (int sp = 0; sp < nspin; sp++) {
       if (!ensure(h, h->d_P[sp], (size_t)n * 8, "P") || !ensure(h, h->d_K[sp], (size_t)n * 8, "K")) return;
       if (!ck(h, cudaMemcpy(h->d_P[sp].p, src[sp], (size_t)n * 8, cudaMemcpyHostToDevice), "P upload")) return;
+      h->h2d_bytes += (long long)n * 8;
       if (!ck(h, cudaMemsetAsync(h->d_K[sp].p, 0, (size_t)n * 8, h->stream), "K zero")) return;
    }
    upload_tables(h);
@@ -441,6 +490,71 @@ static void get_K_impl(Handle *h, double *Ka, double *Kb) {
       if (dst[sp]) ck(h, cudaMemcpy(dst[sp], h->d_K[sp].p, h->FP_size * 8, cudaMemcpyDeviceToHost), "K download");
 }
 
+// Re-run every recorded batch with the current P (K is zeroed first). Returns the elapsed
+// milliseconds measured with CUDA events on the handle's stream.
+static double replay_impl(Handle *h, double *kt) {
+   if (h->err) return -1.0;
+   if (h->recs.empty()) { set_error(h, 4, "libgint_replay: nothing recorded"); return -1.0; }
+   if (!upload_tables(h)) return -1.0;
+   size_t ac = 0, gs = 0;
+   for (auto &rb : h->recs) {
+      ac = std::max(ac, rb.ac_doubles);
+      for (auto &g : rb.segs) { int a, b; gs = std::max(gs, group_global_scratch(h->plans[g.c], &a, &b)); }
+   }
+   if (!ensure(h, h->rec_ac, std::max<size_t>(ac * 8, 256), "replay AC")) return -1.0;
+   if (gs && !ensure(h, h->rec_gscr, gs * 8, "replay HRR scratch")) return -1.0;
+   cudaEvent_t e0, e1;
+   cudaEventCreate(&e0); cudaEventCreate(&e1);
+   DevCtx ctx = make_ctx(h);
+   ck(h, cudaEventRecord(e0, h->stream), "event");
+   for (int sp = 0; sp < h->nspin; sp++) ck(h, cudaMemsetAsync(h->d_K[sp].p, 0, h->FP_size * 8, h->stream), "K zero");
+   // optional per-kernel timing: one event pair per launch, summed per kernel
+   std::vector<cudaEvent_t> kev;
+   auto kmark = [&]() {
+      if (!kt) return;
+      cudaEvent_t e; cudaEventCreate(&e); cudaEventRecord(e, h->stream); kev.push_back(e);
+   };
+   for (auto &rb : h->recs) {
+      char *base = (char *)rb.rec.p;
+      for (auto &g : rb.segs) {
+         BatchArgs bt;
+         std::memset(&bt, 0, sizeof(bt));
+         bt.cls = g.c;
+         bt.plan = (const ClassPlan *)h->d_plans.p + g.c;
+         bt.prm = (const uint32_t *)(base + g.o_prm);
+         bt.prm_shell = (const uint32_t *)(base + g.o_ps);
+         bt.shells = (const ShellRec *)(base + g.o_sh);
+         bt.groups = (const GroupRec *)(base + g.o_g);
+         bt.qrtts = (const QrttRec *)(base + g.o_q);
+         bt.nprm = g.nprm; bt.nshell = g.nshell; bt.ngroup = g.ngroup;
+         bt.AC = (double *)h->rec_ac.p + g.ac_off;
+         bt.gscratch = (double *)h->rec_gscr.p;
+         kmark();
+         if (!ck(h, launch_prim(ctx, bt, h->plans[g.c], h->stream), "k_prim launch")) break;
+         kmark();
+         if (!ck(h, launch_group(ctx, bt, h->plans[g.c], h->stream), "k_group launch")) break;
+         kmark();
+         h->n_launch += 2;
+      }
+   }
+   ck(h, cudaEventRecord(e1, h->stream), "event");
+   ck(h, cudaEventSynchronize(e1), "replay");
+   if (kt) {
+      kt[0] = kt[1] = 0.0;
+      for (size_t i = 0; i + 2 < kev.size(); i += 3) {
+         float a = 0, b = 0;
+         cudaEventElapsedTime(&a, kev[i], kev[i + 1]);
+         cudaEventElapsedTime(&b, kev[i + 1], kev[i + 2]);
+         kt[0] += a; kt[1] += b;
+      }
+      for (auto e : kev) cudaEventDestroy(e);
+   }
+   float ms = -1.f;
+   cudaEventElapsedTime(&ms, e0, e1);
+   cudaEventDestroy(e0); cudaEventDestroy(e1);
+   return h->err ? -1.0 : (double)ms;
+}
+
 }  // namespace gint
 
 using namespace gint;
@@ -452,6 +566,7 @@ extern "C" {
 
 void *libgint_create_handle(void) {
    Handle *h = new Handle();
+   for (int c = 0; c < 256; c++) h->open_of[c] = -1;
    for (int c = 0; c < 256; c++) build_class_plan(c >> 6, (c >> 4) & 3, (c >> 2) & 3, c & 3, h->plans[c]);
    return h;
 }
@@ -591,20 +706,26 @@ void libgint_add_shell(void *hh, int i, int j, int k, int l, int n1, int n2) {
          return;
       }
    }
-   const uint32_t poff = (uint32_t)h->set_prms.size();
    const uint32_t np = (uint32_t)h->prm_tmp.size();
-   h->set_prms.insert(h->set_prms.end(), h->prm_tmp.begin(), h->prm_tmp.end());
-   h->prm_tmp.clear();
    for (int a = 0; a < S4[0]->nL; a++) for (int b = 0; b < S4[1]->nL; b++)
    for (int c = 0; c < S4[2]->nL; c++) for (int d = 0; d < S4[3]->nL; d++) {
-      PendShell ps;
-      ps.cls = cls_of(S4[0]->l[a], S4[1]->l[b], S4[2]->l[c], S4[3]->l[d]);
+      const int cl = cls_of(S4[0]->l[a], S4[1]->l[b], S4[2]->l[c], S4[3]->l[d]);
+      OpenGroup *og = open_group(h, cl);
+      if (!og) { set_error(h, 2, "libgint_add_shell: too many l-combinations in one set quartet"); break; }
+      ClassQ &Q = h->q[cl];
+      ShellRec sr;
       const int li[4] = {a, b, c, d};
-      for (int q = 0; q < 4; q++) ps.ent[q] = (uint32_t)(h->ent_base[idx[q]] + li[q]);
-      ps.n1 = (uint16_t)n1; ps.n2 = (uint16_t)n2;
-      ps.prm_off = poff; ps.nprm = np;
-      h->set_shells.push_back(ps);
+      for (int q = 0; q < 4; q++) sr.ent[q] = (uint32_t)(h->ent_base[idx[q]] + li[q]);
+      sr.prm_off = (uint32_t)Q.prm.size();
+      sr.nprm = np;
+      sr.n1 = (uint16_t)n1; sr.n2 = (uint16_t)n2;
+      sr.group = 0;
+      const uint32_t sid = (uint32_t)Q.shells.size();
+      Q.prm.insert(Q.prm.end(), h->prm_tmp.begin(), h->prm_tmp.end());
+      Q.prm_shell.insert(Q.prm_shell.end(), np, sid);
+      Q.shells.push_back(sr);
    }
+   h->prm_tmp.clear();
 }
 
 void libgint_add_cell(void *hh) { (void)hh; }
@@ -616,10 +737,11 @@ void libgint_add_qrt(void *hh, int la, int lb, int lc, int ld, int nla, int nlb,
       set_error(h, 2, "libgint_add_qrt: l <= 3 and 1 <= nl <= 4");
       return;
    }
-   PendQrt q;
-   q.cls = cls_of(la, lb, lc, ld);
-   q.nl[0] = (uint8_t)nla; q.nl[1] = (uint8_t)nlb; q.nl[2] = (uint8_t)nlc; q.nl[3] = (uint8_t)nld;
-   h->set_qrts.push_back(q);
+   OpenGroup *og = open_group(h, cls_of(la, lb, lc, ld));
+   if (!og) { set_error(h, 2, "libgint_add_qrt: too many l-combinations in one set quartet"); return; }
+   if (og->have_qrt) { set_error(h, 2, "libgint_add_qrt: the same l-combination twice in one set quartet"); return; }
+   og->nl[0] = (uint8_t)nla; og->nl[1] = (uint8_t)nlb; og->nl[2] = (uint8_t)nlc; og->nl[3] = (uint8_t)nld;
+   og->have_qrt = true;
 }
 
 void libgint_add_qrtt(void *hh, double symm_fac, int la, int lb, int lc, int ld, int inla, int inlb, int inlc, int inld,
@@ -637,69 +759,54 @@ void libgint_add_qrtt(void *hh, double symm_fac, int la, int lb, int lc, int ld,
    else if (symm_fac < 0.3) idx_fac = 3;
    else if (symm_fac < 0.75) idx_fac = 2;
    else if (symm_fac < 1.5) idx_fac = 1;
-   PendQrtt q;
-   q.cls = cls_of(la, lb, lc, ld);
-   q.rec.off[0] = off_ac; q.rec.off[1] = off_ad; q.rec.off[2] = off_bc; q.rec.off[3] = off_bd;
-   q.rec.ld[0] = (uint8_t)ld_ac; q.rec.ld[1] = (uint8_t)ld_ad; q.rec.ld[2] = (uint8_t)ld_bc; q.rec.ld[3] = (uint8_t)ld_bd;
-   q.rec.T = (uint8_t)((Tac ? 1 : 0) | (Tad ? 2 : 0) | (Tbc ? 4 : 0) | (Tbd ? 8 : 0));
-   q.rec.idx_fac = (uint8_t)idx_fac;
-   q.rec.pad[0] = q.rec.pad[1] = 0;
-   h->set_qrtts.push_back(q);
+   if (la < 0 || lb < 0 || lc < 0 || ld < 0 || la > kMaxL || lb > kMaxL || lc > kMaxL || ld > kMaxL) {
+      set_error(h, 2, "libgint_add_qrtt: l <= 3");
+      return;
+   }
+   const int cl = cls_of(la, lb, lc, ld);
+   OpenGroup *og = open_group(h, cl);
+   if (!og) { set_error(h, 2, "libgint_add_qrtt: too many l-combinations in one set quartet"); return; }
+   QrttRec r;
+   r.off[0] = off_ac; r.off[1] = off_ad; r.off[2] = off_bc; r.off[3] = off_bd;
+   r.ld[0] = (uint8_t)ld_ac; r.ld[1] = (uint8_t)ld_ad; r.ld[2] = (uint8_t)ld_bc; r.ld[3] = (uint8_t)ld_bd;
+   r.T = (uint8_t)((Tac ? 1 : 0) | (Tad ? 2 : 0) | (Tbc ? 4 : 0) | (Tbd ? 8 : 0));
+   r.idx_fac = (uint8_t)idx_fac;
+   r.pad[0] = r.pad[1] = 0;
+   h->q[cl].qrtts.push_back(r);
+   og->nq++;
 }
 
 void libgint_add_set(void *hh) {
    Handle *h = (Handle *)hh;
-   for (const PendQrt &pq : h->set_qrts) {
-      ClassQ &Q = h->q[pq.cls];
-      GroupRec g;
-      g.shell_off = (uint32_t)Q.shells.size();
-      g.nshell = 0;
-      g.qrtt_off = (uint32_t)Q.qrtts.size();
-      for (int q = 0; q < 4; q++) g.nl[q] = pq.nl[q];
-      const uint32_t gid = (uint32_t)Q.groups.size();
-      size_t added_prims = 0;
-      for (const PendShell &ps : h->set_shells) {
-         if (ps.cls != pq.cls) continue;
-         ShellRec sr;
-         for (int q = 0; q < 4; q++) sr.ent[q] = ps.ent[q];
-         sr.prm_off = (uint32_t)Q.prm.size();
-         sr.nprm = ps.nprm;
-         sr.n1 = ps.n1; sr.n2 = ps.n2;
-         sr.group = gid;
-         const uint32_t sid = (uint32_t)Q.shells.size();
-         Q.prm.insert(Q.prm.end(), h->set_prms.begin() + ps.prm_off, h->set_prms.begin() + ps.prm_off + ps.nprm);
-         Q.prm_shell.insert(Q.prm_shell.end(), ps.nprm, sid);
-         Q.shells.push_back(sr);
-         g.nshell++;
-         added_prims += ps.nprm;
-      }
-      const int nrows = pq.nl[0] * pq.nl[1] * pq.nl[2] * pq.nl[3];
-      int nq = 0;
-      for (const PendQrtt &pt : h->set_qrtts) {
-         if (pt.cls != pq.cls) continue;
-         if (nq < nrows) Q.qrtts.push_back(pt.rec);
-         nq++;
-      }
-      if (g.nshell == 0 || nq != nrows) {
-         // nothing to compute, or an inconsistent set: roll back this group
-         if (g.nshell && nq != nrows) set_error(h, 2, "libgint_add_set: add_qrtt count differs from nla*nlb*nlc*nld");
-         Q.prm.resize(Q.prm.size() - added_prims);
-         Q.prm_shell.resize(Q.prm_shell.size() - added_prims);
-         Q.shells.resize(g.shell_off);
-         Q.qrtts.resize(g.qrtt_off);
+   for (int o = 0; o < h->nopen; o++) {
+      OpenGroup &og = h->open[o];
+      h->open_of[og.cls] = -1;
+      ClassQ &Q = h->q[og.cls];
+      const uint32_t nshell = (uint32_t)Q.shells.size() - og.shell_off;
+      const int nrows = og.nl[0] * og.nl[1] * og.nl[2] * og.nl[3];
+      if (nshell == 0 || !og.have_qrt || og.nq != nrows) {
+         // nothing to compute for this class, or an inconsistent stream: roll the group back
+         if (nshell && (!og.have_qrt || og.nq != nrows))
+            set_error(h, 2, "libgint_add_set: add_qrtt count differs from nla*nlb*nlc*nld");
+         Q.prm.resize(og.prm_off);
+         Q.prm_shell.resize(og.prm_off);
+         Q.shells.resize(og.shell_off);
+         Q.qrtts.resize(og.qrtt_off);
          continue;
       }
+      GroupRec g;
+      g.shell_off = og.shell_off;
+      g.nshell = nshell;
+      g.qrtt_off = og.qrtt_off;
+      for (int q = 0; q < 4; q++) g.nl[q] = og.nl[q];
       Q.groups.push_back(g);
-      if (!Q.active) { Q.active = true; h->active.push_back(pq.cls); }
-      const int S = h->plans[pq.cls].S;
-      h->pend_prims += added_prims;
-      h->pend_ac += added_prims * (size_t)S;
-      h->pend_rec += added_prims * 8 + g.nshell * sizeof(ShellRec) + sizeof(GroupRec) + nrows * sizeof(QrttRec);
+      if (!Q.active) { Q.active = true; h->active.push_back(og.cls); }
+      const size_t added = Q.prm.size() - og.prm_off;
+      h->pend_prims += added;
+      h->pend_ac += added * (size_t)h->plans[og.cls].S;
+      h->pend_rec += added * 8 + nshell * sizeof(ShellRec) + sizeof(GroupRec) + nrows * sizeof(QrttRec);
    }
-   h->set_shells.clear();
-   h->set_prms.clear();
-   h->set_qrts.clear();
-   h->set_qrtts.clear();
+   h->nopen = 0;
    const size_t budget = slot_budget_bytes(h);
    if (h->pend_ac * 8 > budget * 7 / 10 || h->pend_rec > budget * 3 / 10) flush(h);
 }
@@ -708,8 +815,94 @@ void libgint_dispatch(void *hh) { flush((Handle *)hh); }
 
 int libgint_last_error(void *hh) { return ((Handle *)hh)->err; }
 
+// Record the device batches of the following K build(s) so that libgint_replay can recompute
+// K for a new P without the add_* stream (on = 1 starts a new recording, 0 stops).
+void libgint_record(void *hh, int on) {
+   Handle *h = (Handle *)hh;
+   if (on) {
+      drain(h);
+      for (auto &rb : h->recs) release(rb.rec);
+      h->recs.clear();
+   } else {
+      flush(h);
+   }
+   h->recording = on != 0;
+}
+
+double libgint_replay(void *hh) { return replay_impl((Handle *)hh, nullptr); }
+
+// the same with the summed device time of each kernel kind: kt[0] = k_prim, kt[1] = k_group
+double libgint_replay_profile(void *hh, double *kt) { return replay_impl((Handle *)hh, kt); }
+
+// Device event counters per class: [c*4+0] Chebyshev G_m evaluations, [1] Boys evaluations,
+// [2] images through the VRR, [3] primitive quartets (c = la*64+lb*16+lc*4+ld).
+void libgint_set_counters(void *hh, int on) {
+   Handle *h = (Handle *)hh;
+   drain(h);
+   if (on) {
+      if (!ensure(h, h->d_cnt, 256 * 4 * sizeof(unsigned long long), "counters")) return;
+      ck(h, cudaMemset(h->d_cnt.p, 0, 256 * 4 * sizeof(unsigned long long)), "counters");
+   }
+   h->counting = on != 0;
+}
+
+void libgint_get_counters(void *hh, unsigned long long *out) {
+   Handle *h = (Handle *)hh;
+   drain(h);
+   if (!h->d_cnt.p) { std::memset(out, 0, 256 * 4 * sizeof(unsigned long long)); return; }
+   ck(h, cudaMemcpy(out, h->d_cnt.p, 256 * 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost), "counters");
+}
+
+// host-side totals: shells, primitive quartets, groups, flushes, kernel launches
+void libgint_get_stats(void *hh, long long *out) {
+   Handle *h = (Handle *)hh;
+   out[0] = h->n_shells; out[1] = h->n_prims; out[2] = h->n_groups; out[3] = h->n_flush; out[4] = h->n_launch;
+   out[5] = h->h2d_bytes;
+}
+
+double libgint_fp64_peak_tflops(void) { return measure_fp64_peak_tflops(); }
+
 // Sizes of the recursion plan of one class (VRR workspace, contracted targets, HRR workspace,
 // cartesian and spherical block sizes), for inspection and tests.
+// Algorithmic FP64 operation counts of one class, following the reference recursion:
+// out[0] per Chebyshev G_m evaluation, [1] per Boys evaluation, [2] VRR per image,
+// [3] image sum per image (targets), [4] contraction per primitive and contraction row,
+// [5] HRR per shell and contraction row, [6] spherical transform per row, [7] K update per row.
+int libgint_plan_flops(int la, int lb, int lc, int ld, double *out) {
+   ClassPlan p;
+   if (!build_class_plan(la, lb, lc, ld, p)) return 0;
+   auto nc = [](int l) { return (l + 1) * (l + 2) / 2; };
+   const int L = p.L;
+   out[0] = 2.0 * (L + 1) * 105 + 2.0 * (L + 1) * 14 + 4.0 * 13;
+   out[1] = 25.0 + 3.0 * L;
+   double v = 0;
+   for (int b = 1; b < p.nvb; b++) {
+      const VBlock &vb = p.vb[b];
+      double ct;
+      if (vb.c == 0) ct = (vb.a == 1) ? 3 : 7;            // VRR1 / VRR2
+      else if (vb.a == 0) ct = (vb.c == 1) ? 3 : 7;       // VRR3 / VRR4
+      else ct = (vb.c == 1) ? 6 : 10;                     // VRR6 / VRR5
+      v += ct * vb.nelem;
+   }
+   out[2] = v;
+   out[3] = p.S;
+   out[4] = 2.0 * p.S + 3.0;
+   double hrr = 0;
+   for (int o = 0; o < p.nhop; o++) hrr += 2.0 * p.hop[o].nelem;
+   out[5] = hrr;
+   const int dims[4] = {nc(la), nc(lb), nc(lc), nc(ld)}, ls[4] = {la, lb, lc, ld};
+   int cur[4] = {dims[0], dims[1], dims[2], dims[3]};
+   double sph = 0;
+   for (int c = 0; c < 4; c++) {
+      int o[4] = {cur[0], cur[1], cur[2], cur[3]}; o[c] = 2 * ls[c] + 1;
+      sph += 2.0 * o[0] * o[1] * o[2] * o[3] * dims[c];
+      cur[c] = 2 * ls[c] + 1;
+   }
+   out[6] = sph;
+   out[7] = 9.0 * p.Ns;
+   return 1;
+}
+
 int libgint_plan_sizes(int la, int lb, int lc, int ld, int *out) {
    ClassPlan p;
    if (!build_class_plan(la, lb, lc, ld, p)) return 0;
@@ -729,6 +922,8 @@ void libgint_destroy_handle(void *hh) {
       release(s.rec); release(s.ac); release(s.gscr);
       if (s.ev) cudaEventDestroy(s.ev);
    }
+   for (auto &rb : h->recs) release(rb.rec);
+   release(h->rec_ac); release(h->rec_gscr); release(h->d_cnt);
    DBuf *bufs[] = {&h->d_pool, &h->d_ents, &h->d_neighs, &h->d_C0, &h->d_lut, &h->d_bw, &h->d_ft,
                    &h->d_plans, &h->d_err, &h->d_P[0], &h->d_P[1], &h->d_K[0], &h->d_K[1]};
    for (DBuf *b : bufs) release(*b);

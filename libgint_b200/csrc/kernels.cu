@@ -72,14 +72,15 @@ static __device__ void boys_eval(int nmax, double T, double *f, const double *__
 // Truncated-Coulomb G_m(T,R) * Kfac (reference src/t_c_g0_n.cpp:67-180); falls back to the
 // Boys function for R > 11 and T < R^2 - 11 R.
 // ---------------------------------------------------------------------------------------
-static __device__ void fm_eval(const DevCtx &ctx, int L, double R, double T, double Kfac, double *res) {
+// returns 0 when T is beyond the truncation (zeros), 1 for the Chebyshev series, 2 for Boys
+static __device__ int fm_eval(const DevCtx &ctx, int L, double R, double T, double Kfac, double *res) {
    double upper = R * R + 11.0 * R + 50.0;
    double lower = R * R - 11.0 * R + 0.0;
    double X1, X2;
    int patch;
    if (T > upper) {
       for (int n = 0; n <= L; n++) res[n] = 0.0;
-      return;
+      return 0;
    }
    if (R <= 11.0) {
       X2 = R / 11.0;
@@ -93,7 +94,7 @@ static __device__ void fm_eval(const DevCtx &ctx, int L, double R, double T, dou
    } else {
       if (T < lower) {
          boys_eval(L, T, res, ctx.ftable, Kfac);
-         return;
+         return 2;
       }
       X2 = 11.0 / R;
       X1 = (T - lower) / (upper - lower);
@@ -130,6 +131,7 @@ static __device__ void fm_eval(const DevCtx &ctx, int L, double R, double T, dou
       }
       res[k] = tmp * Kfac;
    }
+   return 1;
 }
 
 // minimum-image wrap (reference src/util.cpp:235-265)
@@ -280,6 +282,7 @@ __global__ void __launch_bounds__(256) k_prim(DevCtx ctx, BatchArgs bt, int team
 
       for (int j = lane; j < S; j += TS) acc[j] = 0.0;
       double s00 = 0.0;
+      unsigned c_cheb = 0, c_boys = 0, c_vrr = 0;
       // (ss|ss) needs no VRR: its only target is the image sum of (00|00)
       const bool need_vrr = !(pl->want00 && pl->ntg == 1);
       team_sync<TS>(mask);
@@ -294,7 +297,8 @@ __global__ void __launch_bounds__(256) k_prim(DevCtx ctx, BatchArgs bt, int team
             double PQ0 = P[0] - Q[0] - g0, PQ1 = P[1] - Q[1] - g1, PQ2 = P[2] - Q[2] - g2;
             double rpq2 = (PQ0 * PQ0 + PQ1 * PQ1 + PQ2 * PQ2);
             double T = rho * rpq2;
-            fm_eval(ctx, L, R, T, Kfac, myfm);
+            const int br = fm_eval(ctx, L, R, T, Kfac, myfm);
+            c_cheb += (br == 1); c_boys += (br == 2);
             s00 += myfm[0];
             surv = need_vrr && (myfm[0] > 1.e-12);
          }
@@ -303,6 +307,7 @@ __global__ void __launch_bounds__(256) k_prim(DevCtx ctx, BatchArgs bt, int team
             const int src = __ffs(bal) - 1;
             bal &= bal - 1;
             if (lane == src) {
+               c_vrr++;
                const int n3s = n0 + src;
                const double g0 = __ldg(ctx.neighs + n3s * 3 + 0), g1 = __ldg(ctx.neighs + n3s * 3 + 1),
                             g2 = __ldg(ctx.neighs + n3s * 3 + 2);
@@ -345,6 +350,22 @@ __global__ void __launch_bounds__(256) k_prim(DevCtx ctx, BatchArgs bt, int team
             for (int o = TS / 2; o > 0; o >>= 1) s00 += __shfl_down_sync(mask, s00, o, TS);
          }
          if (lane == 0) acc[pl->s00] += s00;
+      }
+      if (ctx.cnt) {
+         if (TS > 1) {
+#pragma unroll
+            for (int o = TS / 2; o > 0; o >>= 1) {
+               c_cheb += __shfl_down_sync(mask, c_cheb, o, TS);
+               c_boys += __shfl_down_sync(mask, c_boys, o, TS);
+               c_vrr += __shfl_down_sync(mask, c_vrr, o, TS);
+            }
+         }
+         if (lane == 0) {
+            atomicAdd(ctx.cnt + bt.cls * 4 + 0, (unsigned long long)c_cheb);
+            atomicAdd(ctx.cnt + bt.cls * 4 + 1, (unsigned long long)c_boys);
+            atomicAdd(ctx.cnt + bt.cls * 4 + 2, (unsigned long long)c_vrr);
+            atomicAdd(ctx.cnt + bt.cls * 4 + 3, 1ull);
+         }
       }
       team_sync<TS>(mask);
       double *out = bt.AC + (size_t)p * S;
@@ -620,6 +641,46 @@ cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan
       k_group<<<grid, warps * 32, plan_bytes, st>>>(ctx, bt, (int)wd, 1);
    }
    return cudaGetLastError();
+}
+
+// Dependent FMA chains, 8 independent chains per thread: measures the FP64 FMA pipe rate.
+__global__ void k_fp64_fma(double *out, int iters, double a, double b) {
+   double x[8];
+#pragma unroll
+   for (int i = 0; i < 8; i++) x[i] = threadIdx.x * 1e-3 + i;
+   for (int it = 0; it < iters; it++) {
+#pragma unroll
+      for (int i = 0; i < 8; i++) x[i] = fma(x[i], a, b);
+   }
+   double s = 0;
+#pragma unroll
+   for (int i = 0; i < 8; i++) s += x[i];
+   if (s == 12345.678) out[0] = s;   // keeps the chains alive
+}
+
+double measure_fp64_peak_tflops() {
+   int dev = 0, sms = 0;
+   cudaGetDevice(&dev);
+   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+   double *d = nullptr;
+   if (cudaMalloc(&d, 8) != cudaSuccess) return 0.0;
+   const int iters = 4096, threads = 512, blocks = sms * 8;
+   cudaEvent_t e0, e1;
+   cudaEventCreate(&e0); cudaEventCreate(&e1);
+   k_fp64_fma<<<blocks, threads>>>(d, iters, 0.999999, 1e-7);   // warm-up
+   float best = 1e30f;
+   for (int rep = 0; rep < 5; rep++) {
+      cudaEventRecord(e0);
+      k_fp64_fma<<<blocks, threads>>>(d, iters, 0.999999, 1e-7);
+      cudaEventRecord(e1);
+      cudaEventSynchronize(e1);
+      float ms = 0; cudaEventElapsedTime(&ms, e0, e1);
+      best = std::min(best, ms);
+   }
+   cudaEventDestroy(e0); cudaEventDestroy(e1);
+   cudaFree(d);
+   const double flops = 2.0 * 8.0 * iters * (double)threads * blocks;
+   return flops / (best * 1e-3) / 1e12;
 }
 
 }  // namespace gint

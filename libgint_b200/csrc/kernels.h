@@ -26,6 +26,7 @@ struct DevCtx {
    double hf_fac;
    size_t FP_size;
    int *err;
+   unsigned long long *cnt;   // optional event counters per class [256][4], or null
 };
 
 // One class-sorted segment of a batch (device pointers).
@@ -39,6 +40,7 @@ struct BatchArgs {
    uint32_t nprm, nshell, ngroup;
    double *AC;                // [nprm][S] image-summed VRR targets
    double *gscratch;          // HRR workspace in global memory for the largest classes
+   int cls;                   // la*64 + lb*16 + lc*4 + ld
 };
 
 bool build_class_plan(int la, int lb, int lc, int ld, ClassPlan &p);
@@ -47,5 +49,7 @@ cudaError_t launch_prim(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan 
 cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan &hp, cudaStream_t st);
 size_t group_global_scratch(const ClassPlan &hp, int *grid, int *warps);
 int prim_team_size(const ClassPlan &hp);
+// sustained FP64 FMA rate of this GPU (TFLOP/s), from a dependent-FMA kernel
+double measure_fp64_peak_tflops();
 
 }  // namespace gint

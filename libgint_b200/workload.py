@@ -6,6 +6,7 @@ the libgint_* entry points. The named configurations follow the benchmark defini
 
   small_l2      4 water-like molecules, 12 A box, no PBC, l<=2 basis, 20 occupied orbitals
   periodic_l2   32 molecules, 9.86 A cubic cell, 27 images, l<=2, 128 occupied orbitals
+  periodic_l2_small  12 molecules at the same density (7.1 A cell), for kernel profiling
   periodic_l3   64 molecules, 12.4 A cell, 125 images, l<=3 basis with general contraction
 """
 import ctypes
@@ -37,6 +38,7 @@ class GdInfo(ctypes.Structure):
 CONFIGS = {
     "small_l2": dict(n_mol=4, box_ang=12.0, periodic=0, n_img_1d=1, basis=2, n_occ=20),
     "periodic_l2": dict(n_mol=32, box_ang=9.86, periodic=1, n_img_1d=3, basis=2, n_occ=128),
+    "periodic_l2_small": dict(n_mol=12, box_ang=7.1, periodic=1, n_img_1d=3, basis=2, n_occ=48),
     "periodic_l3": dict(n_mol=64, box_ang=12.4, periodic=1, n_img_1d=5, basis=3, n_occ=256),
 }
 
@@ -69,6 +71,11 @@ def driver():
         lib.gd_build_K.restype = ctypes.c_double
         lib.gd_build_K.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _D, _D,
                                    ctypes.c_long, ctypes.c_long, _D]
+        lib.gd_build_K_subset.restype = ctypes.c_double
+        lib.gd_build_K_subset.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _D, _D,
+                                          ctypes.POINTER(ctypes.c_long), ctypes.c_long, _D]
+        lib.gd_get_coeffs.restype = ctypes.c_int
+        lib.gd_get_coeffs.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D, ctypes.POINTER(ctypes.c_int)]
         lib.gd_teardown.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         lib.gd_tcg_table.restype = ctypes.c_int
         lib.gd_tcg_table.argtypes = [ctypes.c_int, _D]
@@ -142,6 +149,12 @@ class Workload:
         driver().gd_get_sets(self._w, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
         return out
 
+    def coeffs(self, s):
+        """(normalised coefficients [nl, np], exponents [np]) of set s."""
+        K = np.zeros(64); Z = np.zeros(16); nl = ctypes.c_int()
+        np_ = driver().gd_get_coeffs(self._w, s, _dp(K), _dp(Z), ctypes.byref(nl))
+        return K[:nl.value * np_].reshape(nl.value, np_), Z[:np_]
+
     def setq(self):
         out = np.empty((self.info["n_setq"], 6), dtype=np.int64)
         driver().gd_get_setq(self._w, out.ctypes.data_as(ctypes.POINTER(ctypes.c_long)))
@@ -177,6 +190,16 @@ class Session:
         t = np.zeros(3)
         Pp = None if P is None else _dp(np.ascontiguousarray(P, dtype=np.float64))
         ms = driver().gd_build_K(self.wl._w, self.api._a, self.h, Pp, _dp(K), q0, q1, _dp(t))
+        return K, ms, t
+
+    def build_K_subset(self, idx, P=None):
+        """K build over the listed set quartets only."""
+        idx = np.ascontiguousarray(idx, dtype=np.int64)
+        K = np.zeros(self.wl.info["flat_size"])
+        t = np.zeros(3)
+        Pp = None if P is None else _dp(np.ascontiguousarray(P, dtype=np.float64))
+        ms = driver().gd_build_K_subset(self.wl._w, self.api._a, self.h, Pp, _dp(K),
+                                        idx.ctypes.data_as(ctypes.POINTER(ctypes.c_long)), idx.size, _dp(t))
         return K, ms, t
 
     def close(self):
