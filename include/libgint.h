@@ -106,6 +106,8 @@ double libgint_replay(void *handle);
 /* libgint_replay with the summed device time per kernel kind: kt[0] = Fm+VRR kernel,
  * kt[1] = contraction+HRR+spherical+K kernel (ms) */
 double libgint_replay_profile(void *handle, double *kt);
+/* libgint_replay_profile plus the per-class split: kcls[c*2 + {0,1}] (ms), c as above */
+double libgint_replay_profile_classes(void *handle, double *kt, double *kcls);
 /* algorithmic FP64 operation counts of class (la,lb,lc,ld) following the reference recursion:
  * out[0] per Chebyshev G_m evaluation, [1] per Boys evaluation, [2] VRR per image, [3] image
  * sum per image, [4] contraction per primitive and row, [5] HRR per shell and row,

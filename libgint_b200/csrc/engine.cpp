@@ -492,7 +492,7 @@ static void get_K_impl(Handle *h, double *Ka, double *Kb) {
 
 // Re-run every recorded batch with the current P (K is zeroed first). Returns the elapsed
 // milliseconds measured with CUDA events on the handle's stream.
-static double replay_impl(Handle *h, double *kt) {
+static double replay_impl(Handle *h, double *kt, double *kcls = nullptr) {
    if (h->err) return -1.0;
    if (h->recs.empty()) { set_error(h, 4, "libgint_replay: nothing recorded"); return -1.0; }
    if (!upload_tables(h)) return -1.0;
@@ -510,6 +510,7 @@ static double replay_impl(Handle *h, double *kt) {
    for (int sp = 0; sp < h->nspin; sp++) ck(h, cudaMemsetAsync(h->d_K[sp].p, 0, h->FP_size * 8, h->stream), "K zero");
    // optional per-kernel timing: one event pair per launch, summed per kernel
    std::vector<cudaEvent_t> kev;
+   std::vector<int> kcl;
    auto kmark = [&]() {
       if (!kt) return;
       cudaEvent_t e; cudaEventCreate(&e); cudaEventRecord(e, h->stream); kev.push_back(e);
@@ -530,6 +531,7 @@ static double replay_impl(Handle *h, double *kt) {
          bt.AC = (double *)h->rec_ac.p + g.ac_off;
          bt.gscratch = (double *)h->rec_gscr.p;
          kmark();
+         if (kt) kcl.push_back(g.c);
          if (!ck(h, launch_prim(ctx, bt, h->plans[g.c], h->stream), "k_prim launch")) break;
          kmark();
          if (!ck(h, launch_group(ctx, bt, h->plans[g.c], h->stream), "k_group launch")) break;
@@ -541,11 +543,13 @@ static double replay_impl(Handle *h, double *kt) {
    ck(h, cudaEventSynchronize(e1), "replay");
    if (kt) {
       kt[0] = kt[1] = 0.0;
+      if (kcls) std::memset(kcls, 0, sizeof(double) * 512);
       for (size_t i = 0; i + 2 < kev.size(); i += 3) {
          float a = 0, b = 0;
          cudaEventElapsedTime(&a, kev[i], kev[i + 1]);
          cudaEventElapsedTime(&b, kev[i + 1], kev[i + 2]);
          kt[0] += a; kt[1] += b;
+         if (kcls) { kcls[kcl[i / 3] * 2] += a; kcls[kcl[i / 3] * 2 + 1] += b; }
       }
       for (auto e : kev) cudaEventDestroy(e);
    }
@@ -833,6 +837,9 @@ double libgint_replay(void *hh) { return replay_impl((Handle *)hh, nullptr); }
 
 // the same with the summed device time of each kernel kind: kt[0] = k_prim, kt[1] = k_group
 double libgint_replay_profile(void *hh, double *kt) { return replay_impl((Handle *)hh, kt); }
+
+// the same with the per-class split: kcls[c*2 + {0,1}] = ms of the two kernels of class c
+double libgint_replay_profile_classes(void *hh, double *kt, double *kcls) { return replay_impl((Handle *)hh, kt, kcls); }
 
 // Device event counters per class: [c*4+0] Chebyshev G_m evaluations, [1] Boys evaluations,
 // [2] images through the VRR, [3] primitive quartets (c = la*64+lb*16+lc*4+ld).
