@@ -120,6 +120,9 @@ void libgint_get_counters(void *handle, unsigned long long *out);
 /* out[0..5] = shell quartets, primitive quartets, groups, batches, kernel launches, bytes
  * copied host -> device */
 void libgint_get_stats(void *handle, long long *out);
+/* the tables the engine builds on the host, for inspection and tests: Boys table [121*28],
+ * c2s [4][70] (per l: rows m, columns cartesian), patch maps [2*128*128], per-patch (B,W) [207*4] */
+void libgint_host_tables(double *ftable, double *c2s, unsigned char *lut, double *bw);
 /* FP64 FMA rate of the current GPU (TFLOP/s), measured by a dependent-FMA kernel */
 double libgint_fp64_peak_tflops(void);
 

@@ -53,6 +53,7 @@ SIGNATURES = {
     "libgint_get_counters": (None, [_V, ctypes.POINTER(ctypes.c_ulonglong)]),
     "libgint_get_stats": (None, [_V, ctypes.POINTER(ctypes.c_longlong)]),
     "libgint_fp64_peak_tflops": (ctypes.c_double, []),
+    "libgint_host_tables": (None, [_D, _D, ctypes.POINTER(ctypes.c_ubyte), _D]),
 }
 
 

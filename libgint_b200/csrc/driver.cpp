@@ -701,6 +701,9 @@ void *gd_setup(const gd_workload *w, gd_api *a, int max_mem_mb) {
 // times[0] = set_P, [1] = stream, [2] = get_K (ms). P == nullptr uses the workload's P.
 static double build_K_impl(const gd_workload *w, gd_api *a, void *h, const double *P, double *K,
                            long q0, long q1, const long *idx, double *times);
+static int g_reverse_prims = 0;
+// replay the primitive quartets of every shell in reverse order (a reordering of the same sums)
+void gd_set_reverse_prims(int on) { g_reverse_prims = on; }
 
 double gd_build_K(const gd_workload *w, gd_api *a, void *h, const double *P, double *K,
                   long q0, long q1, double *times) {
@@ -727,7 +730,8 @@ static double build_K_impl(const gd_workload *w, gd_api *a, void *h, const doubl
       const SetDef *d4[4] = {&w->defs[s4[0]->def], &w->defs[s4[1]->def], &w->defs[s4[2]->def], &w->defs[s4[3]->def]};
       for (uint32_t hs = q.shell_begin; hs < q.shell_end; hs++) {
          const Shell &sh = w->shells[hs];
-         for (uint32_t p = sh.prm_begin; p < sh.prm_end; p++) {
+         for (uint32_t pp = sh.prm_begin; pp < sh.prm_end; pp++) {
+            const uint32_t p = g_reverse_prims ? sh.prm_end - 1 - (pp - sh.prm_begin) : pp;
             uint32_t c = w->prims[p];
             a->prm(h, c >> 24, (c >> 16) & 255, (c >> 8) & 255, c & 255);
          }

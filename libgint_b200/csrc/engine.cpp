@@ -27,23 +27,43 @@ namespace gint {
 // ---------------------------------------------------------------------------------------
 // tables built on the host
 // ---------------------------------------------------------------------------------------
-// Boys table F_m(T), T = 0, 0.1, ..., 12.0 and m = 0..27 (the Taylor table of the
-// reference's fgamma0, src/fgamma.cpp:109-123), from the convergent series
-// F_m(T) = exp(-T) sum_k (2T)^k / ((2m+1)(2m+3)...(2m+2k+1)) in extended precision.
+// Boys table F_m(T), T = 0, 0.1, ..., 12.0 and m = 0..27, the Taylor table of the
+// reference's fgamma0 (src/libGint.cpp:488-497). The values must be the reference's own, not
+// exact ones: its generator (src/fgamma.cpp:53-123, Bessel-function ratios by a continued
+// fraction and a truncated series) is accurate to ~1e-10 for m >= 6, and the engine has to
+// reproduce those values to agree with the reference's K at 1e-12. The steps below are that
+// algorithm: r_{j-1} = -T / ((4j+2) - T r_j) from r_{kmax+9} = 0, then
+// F_n = f/(2n+1) + sum_k f t_k (prod_{j<=k} r_{j-1}) (2k+1)/(2n+1), f = 2 sinh(T/2) e^{-T/2} / T,
+// t_k = t_{k-1} (2n-2k+1)/(2n+2k+1), stopping at the first term below DBL_EPSILON.
+static void boys_reference_values(int nmax, double T, double *f) {
+   const int kmax = 50;
+   double r[kmax + 10];
+   if (T < 1.e-13) {
+      for (int n = 0; n <= nmax; n++) f[n] = 1.0 / (2. * n + 1.);
+      return;
+   }
+   r[kmax + 9] = 0.0;
+   for (int j = kmax + 9; j >= 1; j--) r[j - 1] = -T / ((4. * j + 2.) - T * r[j]);
+   const double factor = 2.0 * std::sinh(0.5 * T) * std::exp(-0.5 * T) / T;
+   for (int n = 0; n <= nmax; n++) {
+      double sumtot = factor / (2. * n + 1.);
+      double term = 1.0;
+      for (int k = 1; k <= kmax; k++) {
+         term = term * (2. * n - 2. * k + 1.) / (2. * n + 2. * k + 1);
+         double p = 1.0;
+         for (int j = 1; j <= k; j++) p = p * r[j - 1];
+         const double sumterm = factor * term * p * (2. * k + 1.) / (2. * n + 1.);
+         if (std::fabs(sumterm) < 2.220446049250313e-16) break;
+         if (k == kmax) break;
+         sumtot = sumtot + sumterm;
+      }
+      f[n] = sumtot;
+   }
+}
+
 static void make_boys_table(std::vector<double> &ft) {
    ft.assign(121 * 28, 0.0);
-   for (int it = 0; it <= 120; it++) {
-      long double T = (long double)it * 0.1L;
-      for (int m = 0; m < 28; m++) {
-         long double term = 1.0L / (2 * m + 1), sum = term;
-         for (int k = 1; k < 400; k++) {
-            term *= 2.0L * T / (2 * m + 2 * k + 1);
-            sum += term;
-            if (term < 1e-22L * sum) break;
-         }
-         ft[it * 28 + m] = (double)(std::exp(-T) * sum);
-      }
-   }
+   for (int it = 0; it <= 120; it++) boys_reference_values(27, (double)it * 0.1, &ft[it * 28]);
 }
 
 // Cartesian -> real solid harmonic coefficients in CP2K's order and normalisation (the
@@ -87,6 +107,37 @@ static void make_c2s(double out[4][70]) {
    }
 }
 
+// Patch maps (low-R, high-R: the patch containing X = i/127 in each dimension, lo < X <= hi)
+// and the per-patch bias/weight (B, W) that map a patch onto [-1, 1]: TG = (2X - B) W.
+static void make_patch_tables(std::vector<uint8_t> &lut, std::vector<double> &bw) {
+   lut.assign(2 * 128 * 128, 0);
+   for (int i1 = 0; i1 < 128; i1++) {
+      double X1 = (double)i1 / 127.0;
+      for (int i2 = 0; i2 < 128; i2++) {
+         double X2 = (double)i2 / 127.0;
+         for (int side = 0; side < 2; side++) {
+            int first = side ? TCG_NPATCH_LOW : 0, last = side ? TCG_NPATCH : TCG_NPATCH_LOW;
+            int found = 0;
+            for (int p = first; p < last; p++) {
+               double lo1 = tcg_patch_rect[p][0] / 128.0, hi1 = tcg_patch_rect[p][1] / 128.0;
+               double lo2 = tcg_patch_rect[p][2] / 128.0, hi2 = tcg_patch_rect[p][3] / 128.0;
+               bool in1 = X1 <= hi1 && (X1 > lo1 || lo1 == 0.0);
+               bool in2 = X2 <= hi2 && (X2 > lo2 || lo2 == 0.0);
+               if (in1 && in2) { found = p; break; }
+            }
+            lut[side * 128 * 128 + i1 * 128 + i2] = (uint8_t)found;
+         }
+      }
+   }
+   bw.assign(TCG_NPATCH * 4, 0.0);
+   for (int p = 0; p < TCG_NPATCH; p++) {
+      bw[p * 4 + 0] = (tcg_patch_rect[p][0] + tcg_patch_rect[p][1]) / 128.0;
+      bw[p * 4 + 1] = 128.0 / (tcg_patch_rect[p][1] - tcg_patch_rect[p][0]);
+      bw[p * 4 + 2] = (tcg_patch_rect[p][2] + tcg_patch_rect[p][3]) / 128.0;
+      bw[p * 4 + 3] = 128.0 / (tcg_patch_rect[p][3] - tcg_patch_rect[p][2]);
+   }
+}
+
 // ---------------------------------------------------------------------------------------
 // handle
 // ---------------------------------------------------------------------------------------
@@ -111,11 +162,45 @@ struct OpenGroup {
    int nq;
 };
 
+// Growable array in pinned host memory (pageable if no device is present), so that a batch is
+// uploaded straight from the queues with cudaMemcpyAsync.
+template <class T>
+struct PVec {
+   T *d = nullptr;
+   size_t n = 0, cap = 0;
+   bool pinned = false;
+   PVec() = default;
+   PVec(const PVec &) = delete;
+   PVec &operator=(const PVec &) = delete;
+   ~PVec() { release(); }
+   void release() {
+      if (d) { if (pinned) cudaFreeHost(d); else std::free(d); }
+      d = nullptr; cap = 0; n = 0;
+   }
+   void reserve(size_t c) {
+      if (c <= cap) return;
+      size_t nc = std::max(c, cap ? cap * 2 : (size_t)16384);
+      T *nd = nullptr;
+      bool pin = cudaHostAlloc((void **)&nd, nc * sizeof(T), cudaHostAllocPortable) == cudaSuccess;
+      if (!pin) { cudaGetLastError(); nd = (T *)std::malloc(nc * sizeof(T)); }
+      if (n) std::memcpy(nd, d, n * sizeof(T));
+      if (d) { if (pinned) cudaFreeHost(d); else std::free(d); }
+      d = nd; cap = nc; pinned = pin;
+   }
+   inline void push_back(const T &x) { if (n == cap) reserve(n + 1); d[n++] = x; }
+   inline void append(const T *x, size_t k) { if (n + k > cap) reserve(n + k); std::memcpy(d + n, x, k * sizeof(T)); n += k; }
+   inline void fill(size_t k, const T &v) { if (n + k > cap) reserve(n + k); for (size_t i = 0; i < k; i++) d[n + i] = v; n += k; }
+   inline size_t size() const { return n; }
+   inline void clear() { n = 0; }
+   inline void resize(size_t k) { if (k > cap) reserve(k); n = k; }
+   inline T *data() { return d; }
+};
+
 struct ClassQ {
-   std::vector<uint32_t> prm, prm_shell;
-   std::vector<ShellRec> shells;
-   std::vector<GroupRec> groups;
-   std::vector<QrttRec> qrtts;
+   PVec<uint32_t> prm, prm_shell;
+   PVec<ShellRec> shells;
+   PVec<GroupRec> groups;
+   PVec<QrttRec> qrtts;
    bool active = false;
 };
 
@@ -125,11 +210,10 @@ struct DBuf {
 };
 
 struct Slot {
-   char *h_stage = nullptr;
-   size_t stage_bytes = 0;
    DBuf rec, ac, gscr;
-   cudaEvent_t ev = nullptr;
-   bool busy = false;
+   cudaEvent_t ev = nullptr;        // all work of the slot's last batch
+   cudaEvent_t ev_copy = nullptr;   // the uploads of the slot's last batch
+   bool busy = false, copy_busy = false;
 };
 
 struct Handle {
@@ -165,7 +249,8 @@ struct Handle {
    OpenGroup open[64];
    int nopen = 0;
    int open_of[256];
-   ClassQ q[256];
+   ClassQ qs[2][256];               // queue sets, one per slot
+   ClassQ *q = qs[0];               // the set being filled
    std::vector<int> active;
    size_t pend_prims = 0, pend_ac = 0, pend_rec = 0;
    Slot slots[2];
@@ -233,33 +318,9 @@ static bool upload_tables(Handle *h) {
    if (!h->plans_ready) {
       if (!ensure(h, h->d_plans, sizeof(ClassPlan) * 256, "plans")) return false;
       if (!ck(h, cudaMemcpy(h->d_plans.p, h->plans, sizeof(ClassPlan) * 256, cudaMemcpyHostToDevice), "plans")) return false;
-      // patch maps and (bias, weight) per patch from the rectangle table
-      std::vector<uint8_t> lut(2 * 128 * 128);
-      for (int i1 = 0; i1 < 128; i1++) {
-         double X1 = (double)i1 / 127.0;
-         for (int i2 = 0; i2 < 128; i2++) {
-            double X2 = (double)i2 / 127.0;
-            for (int side = 0; side < 2; side++) {
-               int first = side ? TCG_NPATCH_LOW : 0, last = side ? TCG_NPATCH : TCG_NPATCH_LOW;
-               int found = 0;
-               for (int p = first; p < last; p++) {
-                  double lo1 = tcg_patch_rect[p][0] / 128.0, hi1 = tcg_patch_rect[p][1] / 128.0;
-                  double lo2 = tcg_patch_rect[p][2] / 128.0, hi2 = tcg_patch_rect[p][3] / 128.0;
-                  bool in1 = X1 <= hi1 && (X1 > lo1 || lo1 == 0.0);
-                  bool in2 = X2 <= hi2 && (X2 > lo2 || lo2 == 0.0);
-                  if (in1 && in2) { found = p; break; }
-               }
-               lut[side * 128 * 128 + i1 * 128 + i2] = (uint8_t)found;
-            }
-         }
-      }
-      std::vector<double> bw(TCG_NPATCH * 4);
-      for (int p = 0; p < TCG_NPATCH; p++) {
-         bw[p * 4 + 0] = (tcg_patch_rect[p][0] + tcg_patch_rect[p][1]) / 128.0;
-         bw[p * 4 + 1] = 128.0 / (tcg_patch_rect[p][1] - tcg_patch_rect[p][0]);
-         bw[p * 4 + 2] = (tcg_patch_rect[p][2] + tcg_patch_rect[p][3]) / 128.0;
-         bw[p * 4 + 3] = 128.0 / (tcg_patch_rect[p][3] - tcg_patch_rect[p][2]);
-      }
+      std::vector<uint8_t> lut;
+      std::vector<double> bw;
+      make_patch_tables(lut, bw);
       std::vector<double> ft;
       make_boys_table(ft);
       if (!ensure(h, h->d_lut, lut.size(), "lut") || !ensure(h, h->d_bw, bw.size() * 8, "bw") ||
@@ -352,26 +413,32 @@ static size_t slot_budget_bytes(Handle *h) {
 
 static inline size_t al16(size_t x) { return (x + 15) & ~(size_t)15; }
 
+static void clear_queues(Handle *h) {
+   for (int c : h->active) {
+      ClassQ &Q = h->q[c];
+      Q.prm.clear(); Q.prm_shell.clear(); Q.shells.clear(); Q.groups.clear(); Q.qrtts.clear();
+      Q.active = false;
+   }
+   h->active.clear();
+   h->pend_prims = h->pend_ac = h->pend_rec = 0;
+}
+
 static void flush(Handle *h) {
    if (h->active.empty()) return;
-   if (h->err) { // drop queued work after an error
-      for (int c : h->active) { ClassQ &Q = h->q[c]; Q.prm.clear(); Q.prm_shell.clear(); Q.shells.clear(); Q.groups.clear(); Q.qrtts.clear(); Q.active = false; }
-      h->active.clear(); h->pend_prims = h->pend_ac = h->pend_rec = 0;
-      return;
-   }
-   if (!upload_tables(h)) return;
-   if (h->nspin == 0 || !h->d_K[0].p) { set_error(h, 4, "work queued before libgint_set_P"); return; }
-   if (!h->have_pot) { set_error(h, 4, "work queued before libgint_set_Potential_Truncated"); return; }
+   if (h->err) { clear_queues(h); return; }   // drop queued work after an error
+   if (!upload_tables(h)) { clear_queues(h); return; }
+   if (h->nspin == 0 || !h->d_K[0].p) { set_error(h, 4, "work queued before libgint_set_P"); clear_queues(h); return; }
+   if (!h->have_pot) { set_error(h, 4, "work queued before libgint_set_Potential_Truncated"); clear_queues(h); return; }
    for (int c : h->active) {
       if (h->ld_C0 < (h->plans[c].L + 1) * 105) {
          set_error(h, 2, "C0 holds fewer derivative orders than la+lb+lc+ld+1");
+         clear_queues(h);
          return;
       }
    }
    Slot &s = h->slots[h->cur];
-   h->cur ^= 1;
    if (s.busy) { ck(h, cudaEventSynchronize(s.ev), "slot wait"); s.busy = false; }
-   // layout of the staging buffer: per class, prm | prm_shell | shells | groups | qrtts
+   // device layout of the batch: per class, prm | prm_shell | shells | groups | qrtts
    struct Seg { int c; size_t o_prm, o_ps, o_sh, o_g, o_q; size_t ac_off; };
    std::vector<Seg> segs;
    size_t off = 0, ac = 0;
@@ -388,23 +455,8 @@ static void flush(Handle *h) {
       ac += ((size_t)Q.prm.size() * h->plans[c].S + 1) & ~(size_t)1;
       segs.push_back(g);
    }
-   if (s.stage_bytes < off) {
-      if (s.h_stage) cudaFreeHost(s.h_stage);
-      s.h_stage = nullptr; s.stage_bytes = 0;
-      size_t want = std::max(off, (size_t)(64u << 20));
-      if (!ck(h, cudaHostAlloc((void **)&s.h_stage, want, cudaHostAllocPortable), "pinned staging")) return;
-      s.stage_bytes = want;
-   }
    if (!ensure(h, s.rec, std::max(off, (size_t)(64u << 20)), "record buffer")) return;
    if (!ensure(h, s.ac, std::max(ac * 8, (size_t)(64u << 20)), "AC buffer")) return;
-   for (const Seg &g : segs) {
-      ClassQ &Q = h->q[g.c];
-      std::memcpy(s.h_stage + g.o_prm, Q.prm.data(), Q.prm.size() * 4);
-      std::memcpy(s.h_stage + g.o_ps, Q.prm_shell.data(), Q.prm_shell.size() * 4);
-      std::memcpy(s.h_stage + g.o_sh, Q.shells.data(), Q.shells.size() * sizeof(ShellRec));
-      std::memcpy(s.h_stage + g.o_g, Q.groups.data(), Q.groups.size() * sizeof(GroupRec));
-      std::memcpy(s.h_stage + g.o_q, Q.qrtts.data(), Q.qrtts.size() * sizeof(QrttRec));
-   }
    char *dev_rec = (char *)s.rec.p;
    Handle::RecBatch *rb = nullptr;
    if (h->recording) {
@@ -414,8 +466,20 @@ static void flush(Handle *h) {
       dev_rec = (char *)rb->rec.p;
       rb->ac_doubles = ac;
    }
-   if (!ck(h, cudaMemcpyAsync(dev_rec, s.h_stage, off, cudaMemcpyHostToDevice, h->stream), "record upload")) return;
+   for (const Seg &g : segs) {
+      ClassQ &Q = h->q[g.c];
+      auto up = [&](size_t o, const void *src, size_t bytes) {
+         return !bytes || ck(h, cudaMemcpyAsync(dev_rec + o, src, bytes, cudaMemcpyHostToDevice, h->stream), "record upload");
+      };
+      if (!up(g.o_prm, Q.prm.data(), Q.prm.size() * 4) || !up(g.o_ps, Q.prm_shell.data(), Q.prm_shell.size() * 4) ||
+          !up(g.o_sh, Q.shells.data(), Q.shells.size() * sizeof(ShellRec)) ||
+          !up(g.o_g, Q.groups.data(), Q.groups.size() * sizeof(GroupRec)) ||
+          !up(g.o_q, Q.qrtts.data(), Q.qrtts.size() * sizeof(QrttRec)))
+         return;
+   }
    h->h2d_bytes += (long long)off;
+   ck(h, cudaEventRecord(s.ev_copy, h->stream), "event record");
+   s.copy_busy = true;
    DevCtx ctx = make_ctx(h);
    for (const Seg &g : segs) {
       ClassQ &Q = h->q[g.c];
@@ -445,14 +509,24 @@ static void flush(Handle *h) {
       h->n_launch += 2;
       if (rb) rb->segs.push_back({g.c, g.o_prm, g.o_ps, g.o_sh, g.o_g, g.o_q, g.ac_off, bt.nprm, bt.nshell, bt.ngroup});
       h->n_prims += bt.nprm; h->n_shells += bt.nshell; h->n_groups += bt.ngroup;
-      Q.prm.clear(); Q.prm_shell.clear(); Q.shells.clear(); Q.groups.clear(); Q.qrtts.clear();
-      Q.active = false;
    }
-   h->active.clear();
-   h->pend_prims = h->pend_ac = h->pend_rec = 0;
    ck(h, cudaEventRecord(s.ev, h->stream), "event record");
    s.busy = true;
    h->n_flush++;
+   // switch to the other queue set; its previous batch must have finished uploading
+   h->active.clear();
+   h->pend_prims = h->pend_ac = h->pend_rec = 0;
+   h->cur ^= 1;
+   h->q = h->qs[h->cur];
+   Slot &o = h->slots[h->cur];
+   if (o.copy_busy) { ck(h, cudaEventSynchronize(o.ev_copy), "queue wait"); o.copy_busy = false; }
+   for (int c = 0; c < 256; c++) {
+      ClassQ &Q = h->q[c];
+      if (Q.prm.size() || Q.shells.size() || Q.qrtts.size() || Q.groups.size()) {
+         Q.prm.clear(); Q.prm_shell.clear(); Q.shells.clear(); Q.groups.clear(); Q.qrtts.clear();
+      }
+      Q.active = false;
+   }
 }
 
 static void drain(Handle *h) {
@@ -470,6 +544,7 @@ static void set_P_impl(Handle *h, int nspin, const double *Pa, const double *Pb,
    // the previous build must be complete before P/K are replaced
    for (Slot &s : h->slots) if (s.busy) { ck(h, cudaEventSynchronize(s.ev), "slot wait"); s.busy = false; }
    ck(h, cudaStreamSynchronize(h->stream), "stream synchronize");
+   for (Slot &s : h->slots) s.copy_busy = false;
    h->nspin = nspin;
    h->FP_size = (size_t)n;
    const double *src[2] = {Pa, Pb};
@@ -579,7 +654,10 @@ void libgint_init(void *hh) {
    Handle *h = (Handle *)hh;
    ck(h, cudaGetDevice(&h->device), "cudaGetDevice");
    if (!h->stream) ck(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream");
-   for (Slot &s : h->slots) if (!s.ev) ck(h, cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming), "event");
+   for (Slot &s : h->slots) {
+      if (!s.ev) ck(h, cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming), "event");
+      if (!s.ev_copy) ck(h, cudaEventCreateWithFlags(&s.ev_copy, cudaEventDisableTiming), "event");
+   }
 }
 
 void libgint_set_Potential_Truncated(void *hh, double R_cut, double *C0, int ld_C0, int C0_size) {
@@ -725,8 +803,8 @@ void libgint_add_shell(void *hh, int i, int j, int k, int l, int n1, int n2) {
       sr.n1 = (uint16_t)n1; sr.n2 = (uint16_t)n2;
       sr.group = 0;
       const uint32_t sid = (uint32_t)Q.shells.size();
-      Q.prm.insert(Q.prm.end(), h->prm_tmp.begin(), h->prm_tmp.end());
-      Q.prm_shell.insert(Q.prm_shell.end(), np, sid);
+      Q.prm.append(h->prm_tmp.data(), np);
+      Q.prm_shell.fill(np, sid);
       Q.shells.push_back(sr);
    }
    h->prm_tmp.clear();
@@ -818,6 +896,22 @@ void libgint_add_set(void *hh) {
 void libgint_dispatch(void *hh) { flush((Handle *)hh); }
 
 int libgint_last_error(void *hh) { return ((Handle *)hh)->err; }
+
+// The tables the engine builds on the host (for tests): Boys table (121*28), c2s for l<=3
+// (4*70, row-major [m][cartesian] per l), patch maps (2*128*128 bytes), per-patch (B,W) (207*4).
+void libgint_host_tables(double *ftable, double *c2s, unsigned char *lut, double *bw) {
+   std::vector<double> ft;
+   make_boys_table(ft);
+   std::memcpy(ftable, ft.data(), ft.size() * 8);
+   double c[4][70];
+   make_c2s(c);
+   std::memcpy(c2s, c, sizeof(c));
+   std::vector<uint8_t> l;
+   std::vector<double> b;
+   make_patch_tables(l, b);
+   std::memcpy(lut, l.data(), l.size());
+   std::memcpy(bw, b.data(), b.size() * 8);
+}
 
 // Record the device batches of the following K build(s) so that libgint_replay can recompute
 // K for a new P without the add_* stream (on = 1 starts a new recording, 0 stops).
@@ -925,9 +1019,9 @@ void libgint_destroy_handle(void *hh) {
    if (!h) return;
    if (h->stream) cudaStreamSynchronize(h->stream);
    for (Slot &s : h->slots) {
-      if (s.h_stage) cudaFreeHost(s.h_stage);
       release(s.rec); release(s.ac); release(s.gscr);
       if (s.ev) cudaEventDestroy(s.ev);
+      if (s.ev_copy) cudaEventDestroy(s.ev_copy);
    }
    for (auto &rb : h->recs) release(rb.rec);
    release(h->rec_ac); release(h->rec_gscr); release(h->d_cnt);

@@ -166,7 +166,10 @@ static __device__ __forceinline__ void shell_geom(const DevCtx &ctx, const Basis
 // One VRR element of block b (reference VRR1..VRR6, src/compute_VRR.cpp:111-345)
 // pqz: PA[3] WP[3] QC[3] WQ[3] i2ab mrab i2cd mrcd i2z
 // ---------------------------------------------------------------------------------------
-static __device__ __forceinline__ void vrr_elem(const VBlock &b, int e, double *ws, const double *pqz) {
+template <int ST>
+static __device__ __forceinline__ void vrr_elem_s(const VBlock &b, int e, double *ws, const double *pqz) {
+   // ws element x lives at ws[x * ST]: ST = 1 for a team-shared workspace, 32 for the
+   // lane-interleaved per-lane workspaces
    const int a = b.a, c = b.c;
    const int na = ncart(a), nc = ncart(c);
    const int k = e % nc, i = (e / nc) % na, mm = e / (nc * na);
@@ -176,38 +179,44 @@ static __device__ __forceinline__ void vrr_elem(const VBlock &b, int e, double *
       const int d = c_cart_dir[a][i];
       const int im = c_cart_dec[a][i][d];
       const int na1 = ncart(a - 1);
-      const double *b1 = ws + b.in1;
-      v = pqz[d] * b1[(m - b.lo1) * na1 + im] + pqz[3 + d] * b1[(m + 1 - b.lo1) * na1 + im];
+      const double *b1 = ws + b.in1 * ST;
+      v = pqz[d * ST] * b1[((m - b.lo1) * na1 + im) * ST] + pqz[(3 + d) * ST] * b1[((m + 1 - b.lo1) * na1 + im) * ST];
       const int ed = c_cart_exp[a][i][d];
       if (ed >= 2) {
          const int iw = c_cart_dec[a - 1][im][d];
          const int na2 = ncart(a - 2);
-         const double *b2 = ws + b.in2;
-         v += (ed - 1) * (pqz[12] * b2[(m - b.lo2) * na2 + iw] + pqz[13] * b2[(m + 1 - b.lo2) * na2 + iw]);
+         const double *b2 = ws + b.in2 * ST;
+         v += (ed - 1) * (pqz[12 * ST] * b2[((m - b.lo2) * na2 + iw) * ST] + pqz[13 * ST] * b2[((m + 1 - b.lo2) * na2 + iw) * ST]);
       }
    } else {
       const int d = c_cart_dir[c][k];
       const int km = c_cart_dec[c][k][d];
       const int nc1 = ncart(c - 1);
-      const double *b1 = ws + b.in1;
-      v = pqz[6 + d] * b1[((m - b.lo1) * na + i) * nc1 + km] + pqz[9 + d] * b1[((m + 1 - b.lo1) * na + i) * nc1 + km];
+      const double *b1 = ws + b.in1 * ST;
+      v = pqz[(6 + d) * ST] * b1[(((m - b.lo1) * na + i) * nc1 + km) * ST] +
+          pqz[(9 + d) * ST] * b1[(((m + 1 - b.lo1) * na + i) * nc1 + km) * ST];
       const int cd = c_cart_exp[c][k][d];
       if (cd >= 2) {
          const int kw = c_cart_dec[c - 1][km][d];
          const int nc2 = ncart(c - 2);
-         const double *b2 = ws + b.in2;
-         v += (cd - 1) * (pqz[14] * b2[((m - b.lo2) * na + i) * nc2 + kw] + pqz[15] * b2[((m + 1 - b.lo2) * na + i) * nc2 + kw]);
+         const double *b2 = ws + b.in2 * ST;
+         v += (cd - 1) * (pqz[14 * ST] * b2[(((m - b.lo2) * na + i) * nc2 + kw) * ST] +
+                          pqz[15 * ST] * b2[(((m + 1 - b.lo2) * na + i) * nc2 + kw) * ST]);
       }
       if (a > 0) {
          const int ad = c_cart_exp[a][i][d];
          if (ad >= 1) {
             const int im = c_cart_dec[a][i][d];
-            const double *b3 = ws + b.in3;
-            v += ad * pqz[16] * b3[((m + 1 - b.lo3) * ncart(a - 1) + im) * nc1 + km];
+            const double *b3 = ws + b.in3 * ST;
+            v += ad * pqz[16 * ST] * b3[(((m + 1 - b.lo3) * ncart(a - 1) + im) * nc1 + km) * ST];
          }
       }
    }
-   ws[b.off + e] = v;
+   ws[(b.off + e) * ST] = v;
+}
+
+static __device__ __forceinline__ void vrr_elem(const VBlock &b, int e, double *ws, const double *pqz) {
+   vrr_elem_s<1>(b, e, ws, pqz);
 }
 
 template <int TS>
@@ -371,6 +380,291 @@ __global__ void __launch_bounds__(256) k_prim(DevCtx ctx, BatchArgs bt, int team
       double *out = bt.AC + (size_t)p * S;
       for (int j = lane; j < S; j += TS) out[j] = acc[j];
       team_sync<TS>(mask);
+   }
+}
+
+// ---------------------------------------------------------------------------------------
+// k_prim2<LANE_VRR>: Fm + VRR + sum over n3, one warp per chunk of primitive quartets with
+// two compaction stages. (1) all (primitive, image) pairs get the cheap truncation test
+// T <= R^2 + 11R + 50 and the passing pairs are queued; (2) the queue is evaluated 32 at a time
+// (G_m by the Chebyshev series or Boys) so that every lane does useful work, and the images with
+// Fm[0] > 1e-12 are queued again; (3) their VRR runs one image per lane (LANE_VRR, small
+// classes, lane-interleaved workspaces) or one image per warp (level-parallel), and the m = 0
+// targets are summed per primitive in shared memory.
+// ---------------------------------------------------------------------------------------
+struct PrimGeo {
+   double P[3], Q[3], PA[3], QC[3];
+   double Kfac, rho, R, zab, zcd, inv_z, i2ab, mrab, i2cd, mrcd, i2z, pad;
+};
+
+template <bool LANE_VRR>
+__global__ void __launch_bounds__(256) k_prim2(DevCtx ctx, BatchArgs bt, int cp, int warp_doubles) {
+   extern __shared__ __align__(16) double smem[];
+   ClassPlan *pl = reinterpret_cast<ClassPlan *>(smem);
+   {
+      const int nwords = (int)(sizeof(ClassPlan) / 4);
+      const int *src = reinterpret_cast<const int *>(bt.plan);
+      int *dst = reinterpret_cast<int *>(smem);
+      for (int w = threadIdx.x; w < nwords; w += blockDim.x) dst[w] = src[w];
+   }
+   __syncthreads();
+   const int plan_doubles = (int)((sizeof(ClassPlan) + 15) / 16) * 2;
+   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+   double *wb = smem + plan_doubles + (size_t)warp * warp_doubles;
+   const int L = pl->L, V = pl->V, S = pl->S, Ng = ctx.Ng;
+   const int LF = L + 1;
+   // per-warp layout
+   PrimGeo *geo = reinterpret_cast<PrimGeo *>(wb);                     // [cp]
+   double *s00 = wb + cp * (sizeof(PrimGeo) / 8);                     // [cp]
+   double *acc = s00 + cp;                                            // [cp][S]
+   int *q1i = reinterpret_cast<int *>(acc + (size_t)cp * S);          // [64] pair index
+   double *q1t = acc + (size_t)cp * S + 32;                           // [64] T
+   int *q2i = reinterpret_cast<int *>(q1t + 64);                      // [64] pair index
+   double *q2f = q1t + 64 + 32;                                       // [64][LF] Fm
+   double *pqz = q2f + 64 * LF;                                       // [17][32] (lane) or [17]
+   double *ws = pqz + (LANE_VRR ? 17 * 32 : 18);                      // [V][32] (lane) or [V]
+   const bool need_vrr = !(pl->want00 && pl->ntg == 1);
+   const unsigned below = (1u << lane) - 1u;
+   unsigned long long c_cheb = 0, c_boys = 0, c_vrr = 0;
+
+   const uint32_t nchunk = (bt.nprm + cp - 1) / cp;
+   for (uint32_t ch = blockIdx.x * nwarp + warp; ch < nchunk; ch += gridDim.x * nwarp) {
+      const uint32_t p0 = ch * cp;
+      const int np = (int)min((uint32_t)cp, bt.nprm - p0);
+      // ---- per-primitive geometry (reference src/compute_Fm.cpp:66-159, :202-210, :281-290)
+      if (lane < np) {
+         const uint32_t p = p0 + lane;
+         const uint32_t code = bt.prm[p];
+         const ShellRec sh = bt.shells[bt.prm_shell[p]];
+         const BasisEnt ea = ctx.ents[sh.ent[0]], eb = ctx.ents[sh.ent[1]];
+         const BasisEnt ec = ctx.ents[sh.ent[2]], ed = ctx.ents[sh.ent[3]];
+         double A[3], B[3], C[3], D[3], CDs[3];
+         shell_geom(ctx, ea, eb, ec, ed, sh.n1, sh.n2, A, B, C, D, CDs);
+         const double za = ctx.pool[ea.z_off + (code >> 24)], zb = ctx.pool[eb.z_off + ((code >> 16) & 255)];
+         const double zc = ctx.pool[ec.z_off + ((code >> 8) & 255)], zd = ctx.pool[ed.z_off + (code & 255)];
+         const double zab = za + zb, inv_zab = 1. / zab, zcd = zc + zd, inv_zcd = 1. / zcd;
+         const double z = zab + zcd, inv_z = 1. / z;
+         double P[3], Q[3], PQs[3], shift[3];
+         for (int q = 0; q < 3; q++) {
+            P[q] = (za * A[q] + zb * B[q]) * inv_zab;
+            Q[q] = (zc * C[q] + zd * D[q]) * inv_zcd;
+         }
+         pbc(Q, P, ctx.cell, PQs);
+         for (int q = 0; q < 3; q++) shift[q] = P[q] - Q[q] - PQs[q];
+         const double normf = 2. * 17.493418327624862 * inv_zab * inv_zcd;
+         double dx = A[0] - B[0], dy = A[1] - B[1], dz = A[2] - B[2];
+         const double RAB2 = dx * dx + dy * dy + dz * dz;
+         const double expon_ab = -(za * zb) / (za + zb) * RAB2;
+         dx = C[0] - D[0]; dy = C[1] - D[1]; dz = C[2] - D[2];
+         const double RCD2 = dx * dx + dy * dy + dz * dz;
+         const double expon_cd = -(zc * zd) / (zc + zd) * RCD2;
+         PrimGeo g;
+         g.Kfac = (1. / sqrt(z)) * normf * exp(expon_ab + expon_cd);
+         double Cs[3], Ds[3];
+         for (int q = 0; q < 3; q++) {
+            Cs[q] = C[q] + shift[q];
+            Ds[q] = C[q] + CDs[q] + __ldg(ctx.neighs + sh.n2 * 3 + q) + shift[q];
+         }
+         for (int q = 0; q < 3; q++) {
+            g.P[q] = P[q];
+            g.Q[q] = (zc * Cs[q] + zd * Ds[q]) * inv_zcd;
+            g.PA[q] = P[q] - A[q];
+            g.QC[q] = g.Q[q] - Cs[q];
+         }
+         g.rho = zab * zcd * inv_z;
+         g.R = ctx.R_cut * sqrt(g.rho);
+         g.zab = zab; g.zcd = zcd; g.inv_z = inv_z;
+         const double izab = 1. / zab, izcd = 1. / zcd;
+         g.i2ab = 0.5 * izab; g.mrab = -1. * g.rho * izab * g.i2ab;
+         g.i2cd = 0.5 * izcd; g.mrcd = -1. * g.rho * izcd * g.i2cd;
+         g.i2z = 0.5 * inv_z; g.pad = 0;
+         geo[lane] = g;
+         s00[lane] = 0.0;
+      }
+      for (int j = lane; j < np * S; j += 32) acc[j] = 0.0;
+      __syncwarp();
+
+      int n1 = 0, n2 = 0;
+      const int npair = np * Ng;
+      // stage 3: VRR of the queued images [0, cnt)
+      auto run_vrr = [&](int cnt) {
+         if (LANE_VRR) {
+            if (lane < cnt) {
+               const int pi = q2i[lane];
+               const int p = pi / Ng, n3 = pi - p * Ng;
+               const PrimGeo &g = geo[p];
+               const double g0 = __ldg(ctx.neighs + n3 * 3 + 0), g1 = __ldg(ctx.neighs + n3 * 3 + 1),
+                            g2 = __ldg(ctx.neighs + n3 * 3 + 2);
+               const double Qp[3] = {g.Q[0] + g0, g.Q[1] + g1, g.Q[2] + g2};
+               double *pz = pqz + lane;
+               for (int q = 0; q < 3; q++) {
+                  const double W = (g.zab * g.P[q] + g.zcd * Qp[q]) * g.inv_z;
+                  pz[q * 32] = g.PA[q];
+                  pz[(3 + q) * 32] = W - g.P[q];
+                  pz[(6 + q) * 32] = g.QC[q];
+                  pz[(9 + q) * 32] = W - Qp[q];
+               }
+               pz[12 * 32] = g.i2ab; pz[13 * 32] = g.mrab; pz[14 * 32] = g.i2cd; pz[15 * 32] = g.mrcd;
+               pz[16 * 32] = g.i2z;
+               double *w = ws + lane;
+               const int n00 = pl->vb[0].nm;
+               for (int q = 0; q < n00; q++) w[q * 32] = q2f[lane * LF + q];
+               for (int bb = 1; bb < pl->nvb; bb++) {
+                  const VBlock vb = pl->vb[bb];
+                  for (int e = 0; e < vb.nelem; e++) vrr_elem_s<32>(vb, e, w, pz);
+               }
+               double *ap = acc + (size_t)p * S;
+               for (int t = 0; t < pl->ntg; t++) {
+                  if (pl->want00 && pl->tg_e[t] == 0 && pl->tg_f[t] == 0) continue;
+                  const double *sp = w + pl->tg_voff[t] * 32;
+                  double *dp = ap + pl->tg_soff[t];
+                  for (int q = 0; q < pl->tg_n[t]; q++) atomicAdd(dp + q, sp[q * 32]);
+               }
+            }
+            __syncwarp();
+         } else {
+            for (int s = 0; s < cnt; s++) {
+               const int pi = q2i[s];
+               const int p = pi / Ng, n3 = pi - p * Ng;
+               const PrimGeo &g = geo[p];
+               if (lane < 3) {
+                  const int q = lane;
+                  const double gq = __ldg(ctx.neighs + n3 * 3 + q);
+                  const double Qp = g.Q[q] + gq;
+                  const double W = (g.zab * g.P[q] + g.zcd * Qp) * g.inv_z;
+                  pqz[q] = g.PA[q]; pqz[3 + q] = W - g.P[q]; pqz[6 + q] = g.QC[q]; pqz[9 + q] = W - Qp;
+               } else if (lane == 3) {
+                  pqz[12] = g.i2ab; pqz[13] = g.mrab; pqz[14] = g.i2cd; pqz[15] = g.mrcd; pqz[16] = g.i2z;
+               }
+               const int n00 = pl->vb[0].nm;
+               for (int q = lane; q < n00; q += 32) ws[q] = q2f[s * LF + q];
+               __syncwarp();
+               for (int lv = 1; lv <= pl->nlev; lv++) {
+                  const int b0 = pl->lev_off[lv - 1], b1 = pl->lev_off[lv];
+                  int tot = 0;
+                  for (int bb = b0; bb < b1; bb++) tot += pl->vb[bb].nelem;
+                  for (int e = lane; e < tot; e += 32) {
+                     int bb = b0, ee = e;
+                     while (ee >= pl->vb[bb].nelem) { ee -= pl->vb[bb].nelem; bb++; }
+                     vrr_elem(pl->vb[bb], ee, ws, pqz);
+                  }
+                  __syncwarp();
+               }
+               double *ap = acc + (size_t)p * S;
+               for (int t = 0; t < pl->ntg; t++) {
+                  if (pl->want00 && pl->tg_e[t] == 0 && pl->tg_f[t] == 0) continue;
+                  const double *sp = ws + pl->tg_voff[t];
+                  double *dp = ap + pl->tg_soff[t];
+                  for (int q = lane; q < pl->tg_n[t]; q += 32) dp[q] += sp[q];
+               }
+               __syncwarp();
+            }
+         }
+      };
+      // stage 2: G_m of the queued pairs [0, cnt), one per lane
+      auto run_fm = [&](int cnt) {
+         bool surv = false;
+         double fm[kMaxLL + 1];
+         int pi = 0;
+         if (lane < cnt) {
+            pi = q1i[lane];
+            const double T = q1t[lane];
+            const int p = pi / Ng;
+            const PrimGeo &g = geo[p];
+            const int br = fm_eval(ctx, L, g.R, T, g.Kfac, fm);
+            c_cheb += (br == 1); c_boys += (br == 2);
+            if (pl->want00) atomicAdd(s00 + p, fm[0]);
+            surv = need_vrr && (fm[0] > 1.e-12);
+         }
+         const unsigned bal = __ballot_sync(0xffffffffu, surv);
+         if (surv) {
+            const int pos = n2 + __popc(bal & below);
+            q2i[pos] = pi;
+            for (int q = 0; q < LF; q++) q2f[pos * LF + q] = fm[q];
+         }
+         n2 += __popc(bal);
+         __syncwarp();
+         const int step = LANE_VRR ? 32 : 1;
+         while (n2 >= step || (n2 > 0 && !LANE_VRR)) {
+            const int cnt2 = LANE_VRR ? 32 : n2;
+            c_vrr += (lane == 0) ? cnt2 : 0;
+            run_vrr(cnt2);
+            // shift the remainder down
+            const int rem = n2 - cnt2;
+            int v = 0;
+            double tmp[kMaxLL + 1];
+            if (lane < rem) {
+               v = q2i[cnt2 + lane];
+               for (int q = 0; q < LF; q++) tmp[q] = q2f[(cnt2 + lane) * LF + q];
+            }
+            __syncwarp();
+            if (lane < rem) {
+               q2i[lane] = v;
+               for (int q = 0; q < LF; q++) q2f[lane * LF + q] = tmp[q];
+            }
+            __syncwarp();
+            n2 = rem;
+         }
+      };
+      // stage 1: truncation test over all (primitive, image) pairs
+      for (int b0 = 0; b0 < npair; b0 += 32) {
+         const int pi = b0 + lane;
+         bool pass = false;
+         double T = 0.0;
+         if (pi < npair) {
+            const int p = pi / Ng, n3 = pi - p * Ng;
+            const PrimGeo &g = geo[p];
+            const double PQ0 = g.P[0] - g.Q[0] - __ldg(ctx.neighs + n3 * 3 + 0);
+            const double PQ1 = g.P[1] - g.Q[1] - __ldg(ctx.neighs + n3 * 3 + 1);
+            const double PQ2 = g.P[2] - g.Q[2] - __ldg(ctx.neighs + n3 * 3 + 2);
+            const double rpq2 = (PQ0 * PQ0 + PQ1 * PQ1 + PQ2 * PQ2);
+            T = g.rho * rpq2;
+            pass = !(T > g.R * g.R + 11.0 * g.R + 50.0);
+         }
+         const unsigned bal = __ballot_sync(0xffffffffu, pass);
+         if (pass) {
+            const int pos = n1 + __popc(bal & below);
+            q1i[pos] = pi;
+            q1t[pos] = T;
+         }
+         n1 += __popc(bal);
+         __syncwarp();
+         if (n1 >= 32) {
+            run_fm(32);
+            const int rem = n1 - 32;
+            int vi = 0; double vt = 0.0;
+            if (lane < rem) { vi = q1i[32 + lane]; vt = q1t[32 + lane]; }
+            __syncwarp();
+            if (lane < rem) { q1i[lane] = vi; q1t[lane] = vt; }
+            __syncwarp();
+            n1 = rem;
+         }
+      }
+      if (n1 > 0) { run_fm(n1); n1 = 0; }
+      if (n2 > 0) {
+         c_vrr += (lane == 0) ? n2 : 0;
+         run_vrr(n2);
+         n2 = 0;
+      }
+      // the (00|00) target collects every image (reference src/compute_VRR.cpp:381-389)
+      if (pl->want00 && lane < np) acc[(size_t)lane * S + pl->s00] += s00[lane];
+      if (lane == 0 && ctx.cnt) atomicAdd(ctx.cnt + bt.cls * 4 + 3, (unsigned long long)np);
+      __syncwarp();
+      double *out = bt.AC + (size_t)p0 * S;
+      for (int j = lane; j < np * S; j += 32) out[j] = acc[j];
+      __syncwarp();
+   }
+   if (ctx.cnt) {
+      for (int o = 16; o > 0; o >>= 1) {
+         c_cheb += __shfl_down_sync(0xffffffffu, c_cheb, o);
+         c_boys += __shfl_down_sync(0xffffffffu, c_boys, o);
+         c_vrr += __shfl_down_sync(0xffffffffu, c_vrr, o);
+      }
+      if (lane == 0) {
+         atomicAdd(ctx.cnt + bt.cls * 4 + 0, c_cheb);
+         atomicAdd(ctx.cnt + bt.cls * 4 + 1, c_boys);
+         atomicAdd(ctx.cnt + bt.cls * 4 + 2, c_vrr);
+      }
    }
 }
 
@@ -595,8 +889,50 @@ int prim_team_size(const ClassPlan &hp) {
    return 32;
 }
 
+// k_prim2 launch shape: primitives per warp chunk and the per-warp shared-memory size
+static void prim2_shape(const ClassPlan &hp, bool lane_vrr, int *cp, size_t *warp_doubles) {
+   int c = std::max(1, std::min(32, 2048 / std::max(1, hp.S)));
+   const size_t geo = (sizeof(PrimGeo) / 8);
+   size_t w = geo * c + c + (size_t)c * hp.S + 32 + 64 + 32 + 64 * (size_t)(hp.L + 1) +
+              (lane_vrr ? 17 * 32 + 32 * (size_t)hp.V : 18 + (size_t)hp.V);
+   *cp = c;
+   *warp_doubles = (w + 1) & ~(size_t)1;
+}
+
+static bool prim2_lane(const ClassPlan &hp) { return hp.V <= 96; }
+
+static int g_prim_kernel = -1;
+
 cudaError_t launch_prim(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan &hp, cudaStream_t st) {
    if (bt.nprm == 0) return cudaSuccess;
+   if (g_prim_kernel < 0) {
+      const char *e = getenv("LIBGINT_PRIM_KERNEL");
+      g_prim_kernel = (e && e[0] == '1') ? 1 : 2;
+   }
+   if (g_prim_kernel == 2) {
+      const bool lane = prim2_lane(hp);
+      int cp = 1;
+      size_t wd = 0;
+      prim2_shape(hp, lane, &cp, &wd);
+      const int budget = std::min(max_dyn_smem(), 200 * 1024);
+      const size_t plan_bytes = (size_t)plan_smem_doubles() * 8;
+      int nw = (int)((budget - (int)plan_bytes) / (wd * 8));
+      nw = std::min(nw, 8);
+      if (nw >= 1) {
+         const size_t smem = plan_bytes + (size_t)nw * wd * 8;
+         const long nchunk = ((long)bt.nprm + cp - 1) / cp;
+         long blocks = std::max(1L, std::min((nchunk + nw - 1) / nw, 148L * 32));
+         if (lane) {
+            cudaFuncSetAttribute(k_prim2<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            k_prim2<true><<<(unsigned)blocks, nw * 32, smem, st>>>(ctx, bt, cp, (int)wd);
+         } else {
+            cudaFuncSetAttribute(k_prim2<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            k_prim2<false><<<(unsigned)blocks, nw * 32, smem, st>>>(ctx, bt, cp, (int)wd);
+         }
+         return cudaGetLastError();
+      }
+      // the largest classes fall through to the team kernel
+   }
    switch (prim_team_size(hp)) {
       case 1: return launch_prim_t<1>(ctx, bt, hp, st);
       case 4: return launch_prim_t<4>(ctx, bt, hp, st);

@@ -36,3 +36,21 @@ def test_flop_model_positive():
     assert lib.libgint_plan_flops(2, 2, 2, 2, fl)
     assert fl[2] > 0 and fl[5] > 0
     assert not lib.libgint_plan_flops(4, 0, 0, 0, fl)
+
+
+def test_engine_host_tables_match_reference():
+    """Boys table, c2s, patch maps and (B,W) that the engine uploads equal the reference's."""
+    from libgint_b200.capi import load_engine
+    lib = load_engine()
+    gold = np.load(os.path.join(GOLDEN, "ref_host_vectors.npz"))
+    ft = np.zeros(121 * 28); c2s = np.zeros(4 * 70); lut = np.zeros(2 * 128 * 128, np.uint8); bw = np.zeros(207 * 4)
+    D = ctypes.POINTER(ctypes.c_double)
+    lib.libgint_host_tables(ft.ctypes.data_as(D), c2s.ctypes.data_as(D),
+                            lut.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)), bw.ctypes.data_as(D))
+    assert np.array_equal(ft, gold["ftable"])
+    assert np.array_equal(lut[:16384], gold["lut_low"]) and np.array_equal(lut[16384:], gold["lut_high"])
+    assert np.array_equal(bw, gold["bw"])
+    off = [0, 1, 10, 40]
+    for l in range(4):
+        nc, ns = (l + 1) * (l + 2) // 2, 2 * l + 1
+        assert np.array_equal(c2s[l * 70:l * 70 + ns * nc], gold["c2s"][off[l]:off[l] + ns * nc]), l
