@@ -613,6 +613,17 @@ int gd_get_coeffs(const gd_workload *w, int s, double *K, double *Z, int *nl) {
    return d.np;
 }
 
+// shells of set quartet q: {n1, n2, n_prims} each; returns the count
+long gd_get_shells(const gd_workload *w, long q, long *out) {
+   const SetQ &s = w->setq[q];
+   long n = 0;
+   for (uint32_t h = s.shell_begin; h < s.shell_end; h++, n++) {
+      out[n * 3 + 0] = w->shells[h].n1; out[n * 3 + 1] = w->shells[h].n2;
+      out[n * 3 + 2] = w->shells[h].prm_end - w->shells[h].prm_begin;
+   }
+   return n;
+}
+
 // per set quartet {i,j,k,l,n_shells,n_prims} (for cost/class statistics)
 void gd_get_setq(const gd_workload *w, long *out) {
    for (size_t q = 0; q < w->setq.size(); q++) {
@@ -702,6 +713,8 @@ void *gd_setup(const gd_workload *w, gd_api *a, int max_mem_mb) {
 static double build_K_impl(const gd_workload *w, gd_api *a, void *h, const double *P, double *K,
                            long q0, long q1, const long *idx, double *times);
 static int g_reverse_prims = 0;
+static long g_only_shell = -1;   // replay only this shell (index within its set quartet), -1: all
+void gd_set_only_shell(long k) { g_only_shell = k; }
 // replay the primitive quartets of every shell in reverse order (a reordering of the same sums)
 void gd_set_reverse_prims(int on) { g_reverse_prims = on; }
 
@@ -729,6 +742,7 @@ static double build_K_impl(const gd_workload *w, gd_api *a, void *h, const doubl
       const Set *s4[4] = {&w->sets[q.i], &w->sets[q.j], &w->sets[q.k], &w->sets[q.l]};
       const SetDef *d4[4] = {&w->defs[s4[0]->def], &w->defs[s4[1]->def], &w->defs[s4[2]->def], &w->defs[s4[3]->def]};
       for (uint32_t hs = q.shell_begin; hs < q.shell_end; hs++) {
+         if (g_only_shell >= 0 && (long)(hs - q.shell_begin) != g_only_shell) continue;
          const Shell &sh = w->shells[hs];
          for (uint32_t pp = sh.prm_begin; pp < sh.prm_end; pp++) {
             const uint32_t p = g_reverse_prims ? sh.prm_end - 1 - (pp - sh.prm_begin) : pp;

@@ -236,6 +236,8 @@ struct Handle {
    // basis
    std::vector<HostSet> sets;
    std::vector<int> ent_base;
+   struct SetFast { int np, nL, l0, ent; };   // hot-path copy of each set's shape
+   std::vector<SetFast> fast;
    bool basis_dirty = true, ent_dirty = true;
    // device-resident data
    DBuf d_pool, d_ents, d_neighs, d_C0, d_lut, d_bw, d_ft, d_plans, d_err;
@@ -377,8 +379,13 @@ static bool upload_tables(Handle *h) {
 static void ensure_ent_base(Handle *h) {
    if (h->ent_base.size() == h->sets.size() && !h->ent_dirty) return;
    h->ent_base.assign(h->sets.size(), 0);
+   h->fast.assign(h->sets.size(), Handle::SetFast{0, 0, 0, 0});
    int n = 0;
-   for (size_t s = 0; s < h->sets.size(); s++) { h->ent_base[s] = n; n += h->sets[s].nL; }
+   for (size_t s = 0; s < h->sets.size(); s++) {
+      h->ent_base[s] = n;
+      h->fast[s] = {h->sets[s].np, h->sets[s].nL, h->sets[s].nL ? h->sets[s].l[0] : 0, n};
+      n += h->sets[s].nL;
+   }
    h->ent_dirty = false;
 }
 
@@ -645,6 +652,7 @@ extern "C" {
 
 void *libgint_create_handle(void) {
    Handle *h = new Handle();
+   h->prm_tmp.reserve(65536);
    for (int c = 0; c < 256; c++) h->open_of[c] = -1;
    for (int c = 0; c < 256; c++) build_class_plan(c >> 6, (c >> 4) & 3, (c >> 2) & 3, c & 3, h->plans[c]);
    return h;
@@ -767,27 +775,58 @@ void libgint_add_prm(void *hh, int ipa, int ipb, int ipc, int ipd) {
    h->prm_tmp.push_back(((uint32_t)ipa << 24) | ((uint32_t)ipb << 16) | ((uint32_t)ipc << 8) | (uint32_t)ipd);
 }
 
+static void add_shell_general(Handle *h, const int idx[4], int n1, int n2);
+
 void libgint_add_shell(void *hh, int i, int j, int k, int l, int n1, int n2) {
    Handle *h = (Handle *)hh;
-   if (h->prm_tmp.empty()) return;
+   const size_t np = h->prm_tmp.size();
+   if (np == 0) return;
    const int ns = (int)h->sets.size();
-   if (i < 0 || j < 0 || k < 0 || l < 0 || i >= ns || j >= ns || k >= ns || l >= ns || n1 < 0 || n2 < 0 ||
-       n1 >= h->Ng || n2 >= h->Ng) {
+   if ((unsigned)i >= (unsigned)ns || (unsigned)j >= (unsigned)ns || (unsigned)k >= (unsigned)ns ||
+       (unsigned)l >= (unsigned)ns || (unsigned)n1 >= (unsigned)h->Ng || (unsigned)n2 >= (unsigned)h->Ng) {
       set_error(h, 2, "libgint_add_shell: set or image index out of range");
       h->prm_tmp.clear();
       return;
    }
    ensure_ent_base(h);
-   const HostSet *S4[4] = {&h->sets[i], &h->sets[j], &h->sets[k], &h->sets[l]};
-   const int idx[4] = {i, j, k, l};
-   for (uint32_t p : h->prm_tmp) {
-      if ((int)(p >> 24) >= S4[0]->np || (int)((p >> 16) & 255) >= S4[1]->np || (int)((p >> 8) & 255) >= S4[2]->np ||
-          (int)(p & 255) >= S4[3]->np) {
-         set_error(h, 2, "libgint_add_prm: primitive index out of range");
-         h->prm_tmp.clear();
-         return;
-      }
+   const Handle::SetFast fa = h->fast[i], fb = h->fast[j], fc = h->fast[k], fd = h->fast[l];
+   // every primitive index must lie inside its set (the kernels index exponents with them)
+   unsigned ma = 0, mb = 0, mc = 0, md = 0;
+   const uint32_t *pc = h->prm_tmp.data();
+   for (size_t p = 0; p < np; p++) {
+      const uint32_t c = pc[p];
+      ma = std::max(ma, c >> 24); mb = std::max(mb, (c >> 16) & 255u);
+      mc = std::max(mc, (c >> 8) & 255u); md = std::max(md, c & 255u);
    }
+   if ((int)ma >= fa.np || (int)mb >= fb.np || (int)mc >= fc.np || (int)md >= fd.np) {
+      set_error(h, 2, "libgint_add_prm: primitive index out of range");
+      h->prm_tmp.clear();
+      return;
+   }
+   if (fa.nL == 1 && fb.nL == 1 && fc.nL == 1 && fd.nL == 1) {
+      const int cl = cls_of(fa.l0, fb.l0, fc.l0, fd.l0);
+      OpenGroup *og = open_group(h, cl);
+      if (!og) { set_error(h, 2, "libgint_add_shell: too many l-combinations in one set quartet"); h->prm_tmp.clear(); return; }
+      ClassQ &Q = h->q[cl];
+      ShellRec sr;
+      sr.ent[0] = (uint32_t)fa.ent; sr.ent[1] = (uint32_t)fb.ent; sr.ent[2] = (uint32_t)fc.ent; sr.ent[3] = (uint32_t)fd.ent;
+      sr.prm_off = (uint32_t)Q.prm.size();
+      sr.nprm = (uint32_t)np;
+      sr.n1 = (uint16_t)n1; sr.n2 = (uint16_t)n2;
+      sr.group = 0;
+      const uint32_t sid = (uint32_t)Q.shells.size();
+      Q.prm.append(pc, np);
+      Q.prm_shell.fill(np, sid);
+      Q.shells.push_back(sr);
+      h->prm_tmp.clear();
+      return;
+   }
+   const int idx[4] = {i, j, k, l};
+   add_shell_general(h, idx, n1, n2);
+}
+
+static void add_shell_general(Handle *h, const int idx[4], int n1, int n2) {
+   const HostSet *S4[4] = {&h->sets[idx[0]], &h->sets[idx[1]], &h->sets[idx[2]], &h->sets[idx[3]]};
    const uint32_t np = (uint32_t)h->prm_tmp.size();
    for (int a = 0; a < S4[0]->nL; a++) for (int b = 0; b < S4[1]->nL; b++)
    for (int c = 0; c < S4[2]->nL; c++) for (int d = 0; d < S4[3]->nL; d++) {

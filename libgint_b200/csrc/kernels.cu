@@ -671,151 +671,179 @@ __global__ void __launch_bounds__(256) k_prim2(DevCtx ctx, BatchArgs bt, int cp,
 // ---------------------------------------------------------------------------------------
 // k_group: contraction + HRR + sum over image pairs + spherical transform + K update
 // ---------------------------------------------------------------------------------------
+// One group (all image pairs of one set quartet, all contraction rows) processed by NL
+// cooperating lanes (NL = 32: one warp; NL = 1: one lane) whose workspace element x lives at
+// ws[x * ST] (ST = 32 for lane-interleaved per-lane workspaces).
+template <int NL, int ST>
+static __device__ __forceinline__ void group_body(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan *pl,
+                                                  const GroupRec &G, double *ws, double *cart, int lane) {
+   const int S = pl->S, Nc = pl->Nc, Ns = pl->Ns;
+   const int la = pl->la, lb = pl->lb, lc = pl->lc, ld = pl->ld;
+   const int nca = ncart(la), ncb = ncart(lb), ncc = ncart(lc), ncd_ = ncart(ld);
+   const int nsa = 2 * la + 1, nsb = 2 * lb + 1, nsc = 2 * lc + 1, nsd = 2 * ld + 1;
+   const int nl1 = G.nl[1], nl2 = G.nl[2], nl3 = G.nl[3];
+   const int nlabcd = G.nl[0] * nl1 * nl2 * nl3;
+   for (int r = 0; r < nlabcd; r++) {
+      const int ia = r / (nl1 * nl2 * nl3), ib = (r / (nl2 * nl3)) % nl1, ic = (r / nl3) % nl2, id = r % nl3;
+      for (int q = lane; q < Nc; q += NL) cart[q * ST] = 0.0;
+      for (uint32_t s = 0; s < G.nshell; s++) {
+         const ShellRec sh = bt.shells[G.shell_off + s];
+         const BasisEnt ea = ctx.ents[sh.ent[0]], eb = ctx.ents[sh.ent[1]];
+         const BasisEnt ec = ctx.ents[sh.ent[2]], ed = ctx.ents[sh.ent[3]];
+         const double *Ka = ctx.pool + ea.k_off + ia * ea.np;
+         const double *Kb = ctx.pool + eb.k_off + ib * eb.np;
+         const double *Kc = ctx.pool + ec.k_off + ic * ec.np;
+         const double *Kd = ctx.pool + ed.k_off + id * ed.np;
+         // contraction over primitives (reference src/compute_ECO.cpp:131-212)
+         for (int j = lane; j < S; j += NL) {
+            double a = 0.0;
+            for (uint32_t ip = 0; ip < sh.nprm; ip++) {
+               const uint32_t code = bt.prm[sh.prm_off + ip];
+               const double kp = __ldg(Ka + (code >> 24)) * __ldg(Kb + ((code >> 16) & 255)) *
+                                 __ldg(Kc + ((code >> 8) & 255)) * __ldg(Kd + (code & 255));
+               a += kp * bt.AC[(size_t)(sh.prm_off + ip) * S + j];
+            }
+            ws[j * ST] = a;
+         }
+         if (NL > 1) __syncwarp();
+         double A[3], B[3], C[3], D[3], CDs[3];
+         shell_geom(ctx, ea, eb, ec, ed, sh.n1, sh.n2, A, B, C, D, CDs);
+         const double AB[3] = {A[0] - B[0], A[1] - B[1], A[2] - B[2]};
+         const double CD[3] = {C[0] - D[0], C[1] - D[1], C[2] - D[2]};
+         // HRR (reference src/compute_HRR.cpp:7-99)
+         for (int lv = 1; lv <= pl->nhlev; lv++) {
+            for (int o = pl->hlev_off[lv - 1]; o < pl->hlev_off[lv]; o++) {
+               const HOp h = pl->hop[o];
+               if (h.type == 0) {
+                  const int c = h.x, d = h.y;
+                  const int nc_ = ncart(c), nd = ncart(d), ncp = ncart(c + 1), ndm = ncart(d - 1);
+                  for (int e = lane; e < h.nelem; e += NL) {
+                     const int l = e % nd, k = (e / nd) % nc_, ie = e / (nd * nc_);
+                     const int dir = c_cart_dir[d][l];
+                     const int lm = c_cart_dec[d][l][dir];
+                     const int kp = c_cart_inc[c][k][dir];
+                     ws[(h.out + e) * ST] = ws[(h.in1 + (ie * ncp + kp) * ndm + lm) * ST] +
+                                            CD[dir] * ws[(h.in2 + (ie * nc_ + k) * ndm + lm) * ST];
+                  }
+               } else {
+                  const int a = h.x, b = h.y;
+                  const int nb = ncart(b), nbm = ncart(b - 1), cdn = ncc * ncd_;
+                  for (int e = lane; e < h.nelem; e += NL) {
+                     const int q = e % cdn, j = (e / cdn) % nb, i = e / (cdn * nb);
+                     const int dir = c_cart_dir[b][j];
+                     const int jm = c_cart_dec[b][j][dir];
+                     const int ip = c_cart_inc[a][i][dir];
+                     ws[(h.out + e) * ST] = ws[(h.in1 + (ip * nbm + jm) * cdn + q) * ST] +
+                                            AB[dir] * ws[(h.in2 + (i * nbm + jm) * cdn + q) * ST];
+                  }
+               }
+            }
+            if (NL > 1) __syncwarp();
+         }
+         for (int q = lane; q < Nc; q += NL) cart[q * ST] += ws[(pl->out_off + q) * ST];
+         if (NL > 1) __syncwarp();
+      }
+      // cartesian -> spherical, one centre at a time (a, b, c, d)
+      {
+         int dims[4] = {nca, ncb, ncc, ncd_};
+         const int ls[4] = {la, lb, lc, ld};
+         const int ns[4] = {nsa, nsb, nsc, nsd};
+         const double *src = cart;
+         for (int ctr = 0; ctr < 4; ctr++) {
+            double *dst = ws + ((ctr & 1) ? Nc * ST : 0);
+            int od[4] = {dims[0], dims[1], dims[2], dims[3]};
+            od[ctr] = ns[ctr];
+            const int tot = od[0] * od[1] * od[2] * od[3];
+            const int nk = dims[ctr];
+            const double *cc = c_c2s[ls[ctr]];
+            int stride = 1;
+            for (int q = ctr + 1; q < 4; q++) stride *= dims[q];
+            for (int t = lane; t < tot; t += NL) {
+               int rem = t, id4[4];
+               for (int q = 3; q >= 0; q--) { id4[q] = rem % od[q]; rem /= od[q]; }
+               const int mi = id4[ctr];
+               id4[ctr] = 0;
+               const int base = ((id4[0] * dims[1] + id4[1]) * dims[2] + id4[2]) * dims[3] + id4[3];
+               double acc = 0.0;
+               for (int k = 0; k < nk; k++) acc += cc[mi * nk + k] * src[(base + k * stride) * ST];
+               dst[t * ST] = acc;
+            }
+            if (NL > 1) __syncwarp();
+            dims[ctr] = ns[ctr];
+            src = dst;
+         }
+      }
+      const double *sph = ws + Nc * ST;   // after 4 passes the result sits in the odd buffer
+      // K update (reference src/compute_KS.cpp:26-115)
+      const QrttRec k = bt.qrtts[G.qrtt_off + r];
+      const double fac = c_symm[k.idx_fac] * ctx.hf_fac;
+      const int nscd = nsc * nsd, nsbcd = nsb * nscd;
+      for (int t = lane; t < Ns; t += NL) {
+         const int isa = t / nsbcd, isb = (t / nscd) % nsb, isc = (t / nsd) % nsc, isd = t % nsd;
+         const int iac = !(k.T & 1) ? isc * k.ld[0] + isa : isa * k.ld[0] + isc;
+         const int iad = !(k.T & 2) ? isd * k.ld[1] + isa : isa * k.ld[1] + isd;
+         const int ibc = !(k.T & 4) ? isc * k.ld[2] + isb : isb * k.ld[2] + isc;
+         const int ibd = !(k.T & 8) ? isd * k.ld[3] + isb : isb * k.ld[3] + isd;
+         const size_t Iac = (size_t)k.off[0] + iac, Iad = (size_t)k.off[1] + iad;
+         const size_t Ibc = (size_t)k.off[2] + ibc, Ibd = (size_t)k.off[3] + ibd;
+         if (Iac >= ctx.FP_size || Iad >= ctx.FP_size || Ibc >= ctx.FP_size || Ibd >= ctx.FP_size) {
+            atomicOr(ctx.err, 1);
+            continue;
+         }
+         const double iabcd = -fac * sph[t * ST];
+         for (int sp = 0; sp < ctx.nspin; sp++) {
+            const double *Pm = ctx.P[sp];
+            double *Km = ctx.K[sp];
+            atomicAdd(Km + Ibd, iabcd * __ldg(Pm + Iac));
+            atomicAdd(Km + Ibc, iabcd * __ldg(Pm + Iad));
+            atomicAdd(Km + Iad, iabcd * __ldg(Pm + Ibc));
+            atomicAdd(Km + Iac, iabcd * __ldg(Pm + Ibd));
+         }
+      }
+      if (NL > 1) __syncwarp();
+   }
+}
+
+static __device__ __forceinline__ void load_plan(const ClassPlan *src_plan, double *smem) {
+   const int nwords = (int)(sizeof(ClassPlan) / 4);
+   const int *src = reinterpret_cast<const int *>(src_plan);
+   int *dst = reinterpret_cast<int *>(smem);
+   for (int w = threadIdx.x; w < nwords; w += blockDim.x) dst[w] = src[w];
+}
+
+// one warp per group
 __global__ void __launch_bounds__(256) k_group(DevCtx ctx, BatchArgs bt, int warp_doubles, int use_global) {
    extern __shared__ __align__(16) double smem[];
-   ClassPlan *pl = reinterpret_cast<ClassPlan *>(smem);
-   {
-      const int nwords = (int)(sizeof(ClassPlan) / 4);
-      const int *src = reinterpret_cast<const int *>(bt.plan);
-      int *dst = reinterpret_cast<int *>(smem);
-      for (int w = threadIdx.x; w < nwords; w += blockDim.x) dst[w] = src[w];
-   }
+   const ClassPlan *pl = reinterpret_cast<const ClassPlan *>(smem);
+   load_plan(bt.plan, smem);
    __syncthreads();
    const int plan_doubles = (int)((sizeof(ClassPlan) + 15) / 16) * 2;
    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32, nwarp = blockDim.x / 32;
    const int gwarp = blockIdx.x * nwarp + warp;
    double *wbase = use_global ? (bt.gscratch + (size_t)gwarp * warp_doubles)
                               : (smem + plan_doubles + (size_t)warp * warp_doubles);
-   const int S = pl->S, Nc = pl->Nc, Ns = pl->Ns;
-   const int Hws = max(pl->H, 2 * Nc);
-   double *ws = wbase;           // HRR workspace (contracted targets first) [Hws]
-   double *cart = wbase + Hws;   // sum over shells [Nc]
-   const int la = pl->la, lb = pl->lb, lc = pl->lc, ld = pl->ld;
-   const int nca = ncart(la), ncb = ncart(lb), ncc = ncart(lc), ncd_ = ncart(ld);
-   const int nsa = 2 * la + 1, nsb = 2 * lb + 1, nsc = 2 * lc + 1, nsd = 2 * ld + 1;
-
+   const int Hws = max(pl->H, 2 * pl->Nc);
    for (uint32_t g = gwarp; g < bt.ngroup; g += gridDim.x * nwarp) {
       const GroupRec G = bt.groups[g];
-      const int nl1 = G.nl[1], nl2 = G.nl[2], nl3 = G.nl[3];
-      const int nlabcd = G.nl[0] * nl1 * nl2 * nl3;
-      for (int r = 0; r < nlabcd; r++) {
-         const int ia = r / (nl1 * nl2 * nl3), ib = (r / (nl2 * nl3)) % nl1, ic = (r / nl3) % nl2, id = r % nl3;
-         for (int q = lane; q < Nc; q += 32) cart[q] = 0.0;
-         for (uint32_t s = 0; s < G.nshell; s++) {
-            const ShellRec sh = bt.shells[G.shell_off + s];
-            const BasisEnt ea = ctx.ents[sh.ent[0]], eb = ctx.ents[sh.ent[1]];
-            const BasisEnt ec = ctx.ents[sh.ent[2]], ed = ctx.ents[sh.ent[3]];
-            const double *Ka = ctx.pool + ea.k_off + ia * ea.np;
-            const double *Kb = ctx.pool + eb.k_off + ib * eb.np;
-            const double *Kc = ctx.pool + ec.k_off + ic * ec.np;
-            const double *Kd = ctx.pool + ed.k_off + id * ed.np;
-            // contraction over primitives (reference src/compute_ECO.cpp:131-212)
-            for (int j = lane; j < S; j += 32) {
-               double a = 0.0;
-               for (uint32_t ip = 0; ip < sh.nprm; ip++) {
-                  const uint32_t code = bt.prm[sh.prm_off + ip];
-                  const double kp = __ldg(Ka + (code >> 24)) * __ldg(Kb + ((code >> 16) & 255)) *
-                                    __ldg(Kc + ((code >> 8) & 255)) * __ldg(Kd + (code & 255));
-                  a += kp * bt.AC[(size_t)(sh.prm_off + ip) * S + j];
-               }
-               ws[j] = a;
-            }
-            __syncwarp();
-            double A[3], B[3], C[3], D[3], CDs[3];
-            shell_geom(ctx, ea, eb, ec, ed, sh.n1, sh.n2, A, B, C, D, CDs);
-            const double AB[3] = {A[0] - B[0], A[1] - B[1], A[2] - B[2]};
-            const double CD[3] = {C[0] - D[0], C[1] - D[1], C[2] - D[2]};
-            // HRR (reference src/compute_HRR.cpp:7-99)
-            for (int lv = 1; lv <= pl->nhlev; lv++) {
-               for (int o = pl->hlev_off[lv - 1]; o < pl->hlev_off[lv]; o++) {
-                  const HOp h = pl->hop[o];
-                  if (h.type == 0) {
-                     const int c = h.x, d = h.y;
-                     const int nc_ = ncart(c), nd = ncart(d), ncp = ncart(c + 1), ndm = ncart(d - 1);
-                     for (int e = lane; e < h.nelem; e += 32) {
-                        const int l = e % nd, k = (e / nd) % nc_, ie = e / (nd * nc_);
-                        const int dir = c_cart_dir[d][l];
-                        const int lm = c_cart_dec[d][l][dir];
-                        const int kp = c_cart_inc[c][k][dir];
-                        ws[h.out + e] = ws[h.in1 + (ie * ncp + kp) * ndm + lm] + CD[dir] * ws[h.in2 + (ie * nc_ + k) * ndm + lm];
-                     }
-                  } else {
-                     const int a = h.x, b = h.y;
-                     const int nb = ncart(b), nbm = ncart(b - 1), cdn = ncc * ncd_;
-                     for (int e = lane; e < h.nelem; e += 32) {
-                        const int q = e % cdn, j = (e / cdn) % nb, i = e / (cdn * nb);
-                        const int dir = c_cart_dir[b][j];
-                        const int jm = c_cart_dec[b][j][dir];
-                        const int ip = c_cart_inc[a][i][dir];
-                        ws[h.out + e] = ws[h.in1 + (ip * nbm + jm) * cdn + q] + AB[dir] * ws[h.in2 + (i * nbm + jm) * cdn + q];
-                     }
-                  }
-               }
-               __syncwarp();
-            }
-            for (int q = lane; q < Nc; q += 32) cart[q] += ws[pl->out_off + q];
-            __syncwarp();
-         }
-         // cartesian -> spherical, one centre at a time (a, b, c, d)
-         {
-            int dims[4] = {nca, ncb, ncc, ncd_};
-            const int ls[4] = {la, lb, lc, ld};
-            const int ns[4] = {nsa, nsb, nsc, nsd};
-            const double *src = cart;
-            for (int ctr = 0; ctr < 4; ctr++) {
-               double *dst = ws + ((ctr & 1) ? Nc : 0);
-               int od[4] = {dims[0], dims[1], dims[2], dims[3]};
-               od[ctr] = ns[ctr];
-               const int tot = od[0] * od[1] * od[2] * od[3];
-               const int nk = dims[ctr];
-               const double *cc = c_c2s[ls[ctr]];
-               int stride = 1;
-               for (int q = ctr + 1; q < 4; q++) stride *= dims[q];
-               for (int t = lane; t < tot; t += 32) {
-                  int rem = t, id4[4];
-                  for (int q = 3; q >= 0; q--) { id4[q] = rem % od[q]; rem /= od[q]; }
-                  const int mi = id4[ctr];
-                  id4[ctr] = 0;
-                  const int base = ((id4[0] * dims[1] + id4[1]) * dims[2] + id4[2]) * dims[3] + id4[3];
-                  double acc = 0.0;
-                  for (int k = 0; k < nk; k++) acc += cc[mi * nk + k] * src[base + k * stride];
-                  dst[t] = acc;
-               }
-               __syncwarp();
-               dims[ctr] = ns[ctr];
-               src = dst;
-            }
-         }
-         const double *sph = ws + Nc;   // after 4 passes the result sits in the odd buffer
-         // K update (reference src/compute_KS.cpp:26-115)
-         const QrttRec k = bt.qrtts[G.qrtt_off + r];
-         const double fac = c_symm[k.idx_fac] * ctx.hf_fac;
-         const int nscd = nsc * nsd, nsbcd = nsb * nscd;
-         for (int t = lane; t < Ns; t += 32) {
-            const int isa = t / nsbcd, isb = (t / nscd) % nsb, isc = (t / nsd) % nsc, isd = t % nsd;
-            const int iac = !(k.T & 1) ? isc * k.ld[0] + isa : isa * k.ld[0] + isc;
-            const int iad = !(k.T & 2) ? isd * k.ld[1] + isa : isa * k.ld[1] + isd;
-            const int ibc = !(k.T & 4) ? isc * k.ld[2] + isb : isb * k.ld[2] + isc;
-            const int ibd = !(k.T & 8) ? isd * k.ld[3] + isb : isb * k.ld[3] + isd;
-            const size_t Iac = (size_t)k.off[0] + iac, Iad = (size_t)k.off[1] + iad;
-            const size_t Ibc = (size_t)k.off[2] + ibc, Ibd = (size_t)k.off[3] + ibd;
-            if (Iac >= ctx.FP_size || Iad >= ctx.FP_size || Ibc >= ctx.FP_size || Ibd >= ctx.FP_size) {
-               atomicOr(ctx.err, 1);
-               continue;
-            }
-            const double iabcd = -fac * sph[t];
-            for (int sp = 0; sp < ctx.nspin; sp++) {
-               const double *Pm = ctx.P[sp];
-               double *Km = ctx.K[sp];
-               atomicAdd(Km + Ibd, iabcd * __ldg(Pm + Iac));
-               atomicAdd(Km + Ibc, iabcd * __ldg(Pm + Iad));
-               atomicAdd(Km + Iad, iabcd * __ldg(Pm + Ibc));
-               atomicAdd(Km + Iac, iabcd * __ldg(Pm + Ibd));
-            }
-         }
-         __syncwarp();
-      }
+      group_body<32, 1>(ctx, bt, pl, G, wbase, wbase + Hws, lane);
    }
+}
+
+// one lane per group, for classes with a small workspace (lane-interleaved in shared memory)
+__global__ void __launch_bounds__(256) k_group_lane(DevCtx ctx, BatchArgs bt, int lane_doubles) {
+   extern __shared__ __align__(16) double smem[];
+   const ClassPlan *pl = reinterpret_cast<const ClassPlan *>(smem);
+   load_plan(bt.plan, smem);
+   __syncthreads();
+   const int plan_doubles = (int)((sizeof(ClassPlan) + 15) / 16) * 2;
+   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32, nwarp = blockDim.x / 32;
+   double *wbase = smem + plan_doubles + (size_t)warp * 32 * lane_doubles + lane;
+   const int Hws = max(pl->H, 2 * pl->Nc);
+   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < bt.ngroup; g += gridDim.x * blockDim.x) {
+      const GroupRec G = bt.groups[g];
+      group_body<1, 32>(ctx, bt, pl, G, wbase, wbase + Hws * 32, 0);
+   }
+   (void)nwarp;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -960,6 +988,18 @@ size_t group_global_scratch(const ClassPlan &hp, int *grid, int *warps) {
 cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan &hp, cudaStream_t st) {
    if (bt.ngroup == 0) return cudaSuccess;
    const size_t wd = group_warp_doubles(hp);
+   if (wd <= 40) {
+      // small workspace: one lane per group, 32 groups per warp
+      const int lane_doubles = (int)wd;
+      const size_t plan_bytes = (size_t)plan_smem_doubles() * 8;
+      const int nw = 8;
+      const size_t smem = plan_bytes + (size_t)nw * 32 * lane_doubles * 8;
+      cudaFuncSetAttribute(k_group_lane, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      long blocks = ((long)bt.ngroup + nw * 32 - 1) / (nw * 32);
+      blocks = std::max(1L, std::min(blocks, 148L * 16));
+      k_group_lane<<<(unsigned)blocks, nw * 32, smem, st>>>(ctx, bt, lane_doubles);
+      return cudaGetLastError();
+   }
    const size_t plan_bytes = (size_t)plan_smem_doubles() * 8;
    const int budget = std::min(max_dyn_smem(), 200 * 1024);
    int nw = (int)((budget - (int)plan_bytes) / (wd * 8));
