@@ -113,6 +113,17 @@ double libgint_replay_profile_classes(void *handle, double *kt, double *kcls);
  * sum per image, [4] contraction per primitive and row, [5] HRR per shell and row,
  * [6] spherical transform per row, [7] K update per row */
 int libgint_plan_flops(int la, int lb, int lc, int ld, double *out);
+/* No counterpart in the reference. For callers that cannot allocate device memory while K is
+ * built (their framework owns every device byte through its own pool, or cudaMalloc/cudaFree
+ * would synchronise a pipeline they must not stall): recompute K from the recorded quartet list
+ * (libgint_record) into the caller's device buffers P_dev/K_dev (K_size doubles, packed like
+ * P), on `stream` (the handle's stream if NULL), with no device allocation. The intermediates
+ * use a fixed 64 MiB device scratch array inside the library, held by every GPU that loads it
+ * until exit; each recorded class segment must fit it (record with a small
+ * libgint_set_max_mem, e.g. 150), otherwise the call fails with a clear error. K_dev is zeroed
+ * first. The first call on a device looks up the scratch address (make it before any stream
+ * capture); calls that overlap on the GPU share the scratch and race. Returns 0 or the error. */
+int libgint_replay_noalloc(void *handle, const double *P_dev, double *K_dev, size_t K_size, void *stream);
 /* per-class device event counters: out[c*4 + {0,1,2,3}] = Chebyshev G_m evaluations, Boys
  * evaluations, images through the VRR, primitive quartets; c = la*64 + lb*16 + lc*4 + ld */
 void libgint_set_counters(void *handle, int on);

@@ -968,6 +968,76 @@ void libgint_record(void *hh, int on) {
 
 double libgint_replay(void *hh) { return replay_impl((Handle *)hh, nullptr); }
 
+// Recompute K from the recorded quartet list into caller-owned device buffers, without any
+// device allocation: the primitive-quartet intermediates and the HRR workspace live in the
+// library's fixed device scratch (64 MiB) instead of buffers allocated by the handle. For
+// callers that cannot call cudaMalloc while building K. Every recorded class segment must fit
+// the scratch (record with a small libgint_set_max_mem, e.g. 150 MB, to keep batches small).
+// K_dev (K_size doubles) is zeroed and then accumulated on `stream` (the handle's stream if
+// null); the call returns after launching. Calls that overlap on the GPU share the scratch and
+// race. The first call on a device looks up the scratch address; make it before any stream
+// capture. Returns 0, or the handle's error code.
+int libgint_replay_noalloc(void *hh, const double *P_dev, double *K_dev, size_t K_size, void *stream) {
+   Handle *h = (Handle *)hh;
+   if (h->err) return h->err;
+   if (h->recs.empty() || !h->plans_ready || h->basis_dirty || h->pot_dirty || h->neighs_dirty || !h->d_err.p) {
+      set_error(h, 4, "libgint_replay_noalloc: record a K build (libgint_record) first");
+      return h->err;
+   }
+   if (!P_dev || !K_dev || K_size == 0) {
+      set_error(h, 2, "libgint_replay_noalloc: P_dev, K_dev and K_size must be given");
+      return h->err;
+   }
+   double *scr = nullptr;
+   if (!ck(h, noalloc_scratch(&scr), "libgint_replay_noalloc: scratch lookup")) return h->err;
+   // every class segment must fit: image-summed targets [nprm][S], then the HRR workspace
+   for (auto &rb : h->recs) {
+      for (auto &g : rb.segs) {
+         const ClassPlan &hp = h->plans[g.c];
+         int a = 0, b = 0;
+         const size_t ac = ((size_t)g.nprm * hp.S + 31) & ~(size_t)31;
+         const size_t need = ac + group_global_scratch(hp, &a, &b);
+         if (need > kNoAllocScratchDoubles) {
+            char msg[256];
+            std::snprintf(msg, sizeof(msg), "libgint_replay_noalloc: a recorded batch of class (%d%d|%d%d) needs %zu "
+                          "doubles of scratch, the maximum is %zu; record with a smaller libgint_set_max_mem",
+                          g.c >> 6, (g.c >> 4) & 3, (g.c >> 2) & 3, g.c & 3, need, kNoAllocScratchDoubles);
+            set_error(h, 5, msg);
+            return h->err;
+         }
+      }
+   }
+   cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+   DevCtx ctx = make_ctx(h);
+   ctx.nspin = 1;
+   ctx.P[0] = P_dev; ctx.P[1] = nullptr;
+   ctx.K[0] = K_dev; ctx.K[1] = nullptr;
+   ctx.FP_size = K_size;
+   ctx.cnt = nullptr;
+   if (!ck(h, cudaMemsetAsync(K_dev, 0, K_size * 8, st), "libgint_replay_noalloc: K zero")) return h->err;
+   for (auto &rb : h->recs) {
+      char *base = (char *)rb.rec.p;
+      for (auto &g : rb.segs) {
+         const ClassPlan &hp = h->plans[g.c];
+         BatchArgs bt;
+         std::memset(&bt, 0, sizeof(bt));
+         bt.cls = g.c;
+         bt.plan = (const ClassPlan *)h->d_plans.p + g.c;
+         bt.prm = (const uint32_t *)(base + g.o_prm);
+         bt.prm_shell = (const uint32_t *)(base + g.o_ps);
+         bt.shells = (const ShellRec *)(base + g.o_sh);
+         bt.groups = (const GroupRec *)(base + g.o_g);
+         bt.qrtts = (const QrttRec *)(base + g.o_q);
+         bt.nprm = g.nprm; bt.nshell = g.nshell; bt.ngroup = g.ngroup;
+         bt.AC = scr;                                                   // segments run in stream order
+         bt.gscratch = scr + (((size_t)g.nprm * hp.S + 31) & ~(size_t)31);
+         if (!ck(h, launch_prim(ctx, bt, hp, st), "libgint_replay_noalloc: k_prim launch")) return h->err;
+         if (!ck(h, launch_group(ctx, bt, hp, st), "libgint_replay_noalloc: k_group launch")) return h->err;
+      }
+   }
+   return 0;
+}
+
 // the same with the summed device time of each kernel kind: kt[0] = k_prim, kt[1] = k_group
 double libgint_replay_profile(void *hh, double *kt) { return replay_impl((Handle *)hh, kt); }
 

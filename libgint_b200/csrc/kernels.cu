@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cstdint>
+#include <mutex>
 #include "engine_types.h"
 #include "kernels.h"
 
@@ -1057,6 +1058,35 @@ double measure_fp64_peak_tflops() {
    cudaFree(d);
    const double flops = 2.0 * 8.0 * iters * (double)threads * blocks;
    return flops / (best * 1e-3) / 1e12;
+}
+
+// ---------------------------------------------------------------------------------------
+// Fixed device scratch for libgint_replay_noalloc. Callers that cannot allocate device
+// memory at K-build time (a framework that owns every device byte through its own pool, or
+// code that must not trigger the implicit synchronisation of cudaMalloc/cudaFree) use this
+// array instead of the handle's allocated AC/HRR buffers. It is a file-scope device array of
+// kNoAllocScratchDoubles doubles (64 MiB) that every GPU which loads the library holds until
+// the process exits. Host code cannot use the name g_noalloc_scratch as a device address; the
+// address is obtained once per device with cudaGetSymbolAddress, with that device current.
+// ---------------------------------------------------------------------------------------
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
+
+cudaError_t noalloc_scratch(double **ptr) {
+   static std::mutex mu;
+   static double *addr[kMaxDevices] = {nullptr};
+   int dev = 0;
+   cudaError_t e = cudaGetDevice(&dev);
+   if (e != cudaSuccess) return e;
+   if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+   std::lock_guard<std::mutex> lock(mu);
+   if (!addr[dev]) {
+      double *p = nullptr;
+      e = cudaGetSymbolAddress((void **)&p, g_noalloc_scratch);
+      if (e != cudaSuccess) return e;
+      addr[dev] = p;
+   }
+   *ptr = addr[dev];
+   return cudaSuccess;
 }
 
 }  // namespace gint

@@ -49,6 +49,11 @@ cudaError_t launch_prim(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan 
 cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan &hp, cudaStream_t st);
 size_t group_global_scratch(const ClassPlan &hp, int *grid, int *warps);
 int prim_team_size(const ClassPlan &hp);
+// Fixed device scratch (file-scope device array in kernels.cu) used by libgint_replay_noalloc:
+// its device address for the current device; the first call on a device looks it up.
+constexpr size_t kNoAllocScratchDoubles = (size_t)8 * 1024 * 1024;   // 64 MiB
+constexpr int kMaxDevices = 64;
+cudaError_t noalloc_scratch(double **ptr);
 // sustained FP64 FMA rate of this GPU (TFLOP/s), from a dependent-FMA kernel
 double measure_fp64_peak_tflops();
 
