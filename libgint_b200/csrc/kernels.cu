@@ -70,13 +70,128 @@ static __device__ void boys_eval(int nmax, double T, double *f, const double *__
 }
 
 // ---------------------------------------------------------------------------------------
+// Geometry that feeds discrete decisions. The minimum-image rounding (which lattice shift
+// brings Q next to P, and so which 27 images the image sum covers), the truncation test, the
+// Boys/Chebyshev branch and the patch index all compare rounded doubles against thresholds;
+// a one-ulp difference can flip them and change K by far more than one ulp. These values are
+// therefore evaluated with explicitly rounded operations in the source's order, with an FMA
+// only where the reference's CUDA build contracts one (the weighted distance), so every
+// decision is the one the reference makes on the same inputs.
+// ---------------------------------------------------------------------------------------
+static __device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+static __device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a, b); }
+static __device__ __forceinline__ double rsub(double a, double b) { return __dsub_rn(a, b); }
+static __device__ __forceinline__ double rdot3(double a0, double b0, double a1, double b1, double a2, double b2) {
+   return radd(radd(rmul(a0, b0), rmul(a1, b1)), rmul(a2, b2));
+}
+// weighted distance (c1 x1 + c2 x2) c12 (reference src/util.h:62-68) as the reference's CUDA
+// build evaluates it: the first product contracted into the sum, fma(c1, x1, c2 x2) c12. This
+// rounding decides the minimum image of P - Q when P - Q lies on half a lattice vector, which
+// happens for symmetric quartets such as (ab|ab') with b' an image of b and equal exponents.
+static __device__ __forceinline__ double wdist(double c1, double x1, double c2, double x2, double c12) {
+   return rmul(__fma_rn(c1, x1, rmul(c2, x2)), c12);
+}
+
+// minimum-image wrap (reference src/util.cpp:132-162)
+static __device__ __forceinline__ void pbc(const double *A, const double *B, const double *cell, double *AB) {
+   const double *hm = cell, *hi = cell + 9;
+   AB[0] = rsub(B[0], A[0]); AB[1] = rsub(B[1], A[1]); AB[2] = rsub(B[2], A[2]);
+   double s0 = rdot3(hi[0], AB[0], hi[3], AB[1], hi[6], AB[2]);
+   double s1 = rdot3(hi[1], AB[0], hi[4], AB[1], hi[7], AB[2]);
+   double s2 = rdot3(hi[2], AB[0], hi[5], AB[1], hi[8], AB[2]);
+   s0 = rsub(s0, round(s0)); s1 = rsub(s1, round(s1)); s2 = rsub(s2, round(s2));
+   AB[0] = rdot3(hm[0], s0, hm[3], s1, hm[6], s2);
+   AB[1] = rdot3(hm[1], s0, hm[4], s1, hm[7], s2);
+   AB[2] = rdot3(hm[2], s0, hm[5], s1, hm[8], s2);
+}
+
+// shell geometry: A, B (image n1), C, D (image n2) as the reference places them
+static __device__ __forceinline__ void shell_geom(const DevCtx &ctx, const BasisEnt &ea, const BasisEnt &eb,
+                                                  const BasisEnt &ec, const BasisEnt &ed, int n1, int n2,
+                                                  double *A, double *B, double *C, double *D, double *CDs) {
+   double ABs[3];
+   pbc(ea.R, eb.R, ctx.cell, ABs);
+   pbc(ec.R, ed.R, ctx.cell, CDs);
+   for (int q = 0; q < 3; q++) {
+      A[q] = ea.R[q];
+      B[q] = radd(radd(ea.R[q], ABs[q]), __ldg(ctx.neighs + n1 * 3 + q));
+      C[q] = ec.R[q];
+      D[q] = radd(radd(ec.R[q], CDs[q]), __ldg(ctx.neighs + n2 * 3 + q));
+   }
+}
+
+// Per-primitive-quartet quantities shared by every image n3.
+struct PrimGeo {
+   double P[3], Q[3], PA[3], QC[3];
+   double Kfac, rho, R, zab, zcd, inv_z, i2ab, mrab, i2cd, mrcd, i2z, pad;
+};
+
+// prepare_Fm and the image-independent part of compute_Vm (reference
+// src/compute_Fm.cpp:66-159, :202-210, :281-290). Q is the ket centre shifted by the
+// minimum-image lattice vector of P - Q, so that image n3 sits at Q + neighs[n3].
+static __device__ __forceinline__ void prim_geometry(const DevCtx &ctx, const ShellRec &sh, uint32_t code,
+                                                     PrimGeo &g) {
+   const BasisEnt ea = ctx.ents[sh.ent[0]], eb = ctx.ents[sh.ent[1]];
+   const BasisEnt ec = ctx.ents[sh.ent[2]], ed = ctx.ents[sh.ent[3]];
+   double A[3], B[3], C[3], D[3], CDs[3];
+   shell_geom(ctx, ea, eb, ec, ed, sh.n1, sh.n2, A, B, C, D, CDs);
+   const double za = ctx.pool[ea.z_off + (code >> 24)], zb = ctx.pool[eb.z_off + ((code >> 16) & 255)];
+   const double zc = ctx.pool[ec.z_off + ((code >> 8) & 255)], zd = ctx.pool[ed.z_off + (code & 255)];
+   const double zab = za + zb, inv_zab = 1. / zab, zcd = zc + zd, inv_zcd = 1. / zcd;
+   const double z = zab + zcd, inv_z = 1. / z;
+   double P[3], Q[3], PQs[3], shift[3];
+   for (int q = 0; q < 3; q++) {
+      P[q] = wdist(za, A[q], zb, B[q], inv_zab);
+      Q[q] = wdist(zc, C[q], zd, D[q], inv_zcd);
+   }
+   pbc(Q, P, ctx.cell, PQs);
+   for (int q = 0; q < 3; q++) shift[q] = rsub(rsub(P[q], Q[q]), PQs[q]);
+   const double normf = 2. * 17.493418327624862 * inv_zab * inv_zcd;   // 2 pi^(5/2) / (zab zcd)
+   double dx = A[0] - B[0], dy = A[1] - B[1], dz = A[2] - B[2];
+   const double RAB2 = dx * dx + dy * dy + dz * dz;
+   const double expon_ab = -(za * zb) / (za + zb) * RAB2;
+   dx = C[0] - D[0]; dy = C[1] - D[1]; dz = C[2] - D[2];
+   const double RCD2 = dx * dx + dy * dy + dz * dz;
+   const double expon_cd = -(zc * zd) / (zc + zd) * RCD2;
+   g.Kfac = (1. / sqrt(z)) * normf * exp(expon_ab + expon_cd);
+   for (int q = 0; q < 3; q++) {
+      const double Cs = radd(C[q], shift[q]);
+      const double Ds = radd(radd(radd(C[q], CDs[q]), __ldg(ctx.neighs + sh.n2 * 3 + q)), shift[q]);
+      g.P[q] = P[q];
+      g.Q[q] = wdist(zc, Cs, zd, Ds, inv_zcd);
+      g.PA[q] = P[q] - A[q];
+      g.QC[q] = g.Q[q] - Cs;
+   }
+   g.rho = rmul(rmul(zab, zcd), inv_z);
+   g.R = rmul(ctx.R_cut, sqrt(g.rho));
+   g.zab = zab; g.zcd = zcd; g.inv_z = inv_z;
+   const double izab = 1. / zab, izcd = 1. / zcd;
+   g.i2ab = 0.5 * izab; g.mrab = -1. * g.rho * izab * g.i2ab;
+   g.i2cd = 0.5 * izcd; g.mrcd = -1. * g.rho * izcd * g.i2cd;
+   g.i2z = 0.5 * inv_z; g.pad = 0;
+}
+
+// T = rho |P - Q - neighs[n3]|^2 (reference src/compute_Fm.cpp:204-210)
+static __device__ __forceinline__ double image_T(const DevCtx &ctx, const PrimGeo &g, int n3) {
+   const double PQ0 = rsub(rsub(g.P[0], g.Q[0]), __ldg(ctx.neighs + n3 * 3 + 0));
+   const double PQ1 = rsub(rsub(g.P[1], g.Q[1]), __ldg(ctx.neighs + n3 * 3 + 1));
+   const double PQ2 = rsub(rsub(g.P[2], g.Q[2]), __ldg(ctx.neighs + n3 * 3 + 2));
+   return rmul(g.rho, rdot3(PQ0, PQ0, PQ1, PQ1, PQ2, PQ2));
+}
+
+// the truncation bound R^2 + 11 R + 50 (reference src/t_c_g0_n.cpp:78)
+static __device__ __forceinline__ double trunc_upper(double R) {
+   return radd(radd(rmul(R, R), rmul(11.0, R)), 50.0);
+}
+
+// ---------------------------------------------------------------------------------------
 // Truncated-Coulomb G_m(T,R) * Kfac (reference src/t_c_g0_n.cpp:67-180); falls back to the
 // Boys function for R > 11 and T < R^2 - 11 R.
 // ---------------------------------------------------------------------------------------
 // returns 0 when T is beyond the truncation (zeros), 1 for the Chebyshev series, 2 for Boys
 static __device__ int fm_eval(const DevCtx &ctx, int L, double R, double T, double Kfac, double *res) {
-   double upper = R * R + 11.0 * R + 50.0;
-   double lower = R * R - 11.0 * R + 0.0;
+   double upper = trunc_upper(R);
+   double lower = radd(rsub(rmul(R, R), rmul(11.0, R)), 0.0);
    double X1, X2;
    int patch;
    if (T > upper) {
@@ -85,9 +200,8 @@ static __device__ int fm_eval(const DevCtx &ctx, int L, double R, double T, doub
    }
    if (R <= 11.0) {
       X2 = R / 11.0;
-      upper = R * R + 11.0 * R + 50.0;
       lower = 0.0;
-      X1 = (T - lower) / (upper - lower);
+      X1 = rsub(T, lower) / rsub(upper, lower);
       int i1 = (int)(X1 * 128), i2 = (int)(X2 * 128);
       if (i1 == 128) i1 = 127;
       if (i2 == 128) i2 = 127;
@@ -98,7 +212,7 @@ static __device__ int fm_eval(const DevCtx &ctx, int L, double R, double T, doub
          return 2;
       }
       X2 = 11.0 / R;
-      X1 = (T - lower) / (upper - lower);
+      X1 = rsub(T, lower) / rsub(upper, lower);
       int i1 = (int)(X1 * 128), i2 = (int)(X2 * 128);
       if (i1 == 128) i1 = 127;
       if (i2 == 128) i2 = 127;
@@ -133,34 +247,6 @@ static __device__ int fm_eval(const DevCtx &ctx, int L, double R, double T, doub
       res[k] = tmp * Kfac;
    }
    return 1;
-}
-
-// minimum-image wrap (reference src/util.cpp:235-265)
-static __device__ __forceinline__ void pbc(const double *A, const double *B, const double *cell, double *AB) {
-   const double *hm = cell, *hi = cell + 9;
-   AB[0] = B[0] - A[0]; AB[1] = B[1] - A[1]; AB[2] = B[2] - A[2];
-   double s0 = hi[0] * AB[0] + hi[3] * AB[1] + hi[6] * AB[2];
-   double s1 = hi[1] * AB[0] + hi[4] * AB[1] + hi[7] * AB[2];
-   double s2 = hi[2] * AB[0] + hi[5] * AB[1] + hi[8] * AB[2];
-   s0 -= round(s0); s1 -= round(s1); s2 -= round(s2);
-   AB[0] = hm[0] * s0 + hm[3] * s1 + hm[6] * s2;
-   AB[1] = hm[1] * s0 + hm[4] * s1 + hm[7] * s2;
-   AB[2] = hm[2] * s0 + hm[5] * s1 + hm[8] * s2;
-}
-
-// shell geometry: A, B (image n1), C, D (image n2) as the reference places them
-static __device__ __forceinline__ void shell_geom(const DevCtx &ctx, const BasisEnt &ea, const BasisEnt &eb,
-                                                  const BasisEnt &ec, const BasisEnt &ed, int n1, int n2,
-                                                  double *A, double *B, double *C, double *D, double *CDs) {
-   double ABs[3];
-   pbc(ea.R, eb.R, ctx.cell, ABs);
-   pbc(ec.R, ed.R, ctx.cell, CDs);
-   for (int q = 0; q < 3; q++) {
-      A[q] = ea.R[q];
-      B[q] = ea.R[q] + ABs[q] + __ldg(ctx.neighs + n1 * 3 + q);
-      C[q] = ec.R[q];
-      D[q] = ec.R[q] + CDs[q] + __ldg(ctx.neighs + n2 * 3 + q);
-   }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -251,44 +337,8 @@ __global__ void __launch_bounds__(256) k_prim(DevCtx ctx, BatchArgs bt, int team
    const unsigned mask = (TS >= 32) ? 0xffffffffu : (((1u << TS) - 1u) << wl);
 
    for (uint32_t p = blockIdx.x * nteam + team; p < bt.nprm; p += gridDim.x * nteam) {
-      const uint32_t code = bt.prm[p];
-      const ShellRec sh = bt.shells[bt.prm_shell[p]];
-      const BasisEnt ea = ctx.ents[sh.ent[0]], eb = ctx.ents[sh.ent[1]];
-      const BasisEnt ec = ctx.ents[sh.ent[2]], ed = ctx.ents[sh.ent[3]];
-      const int ipa = code >> 24, ipb = (code >> 16) & 255, ipc = (code >> 8) & 255, ipd = code & 255;
-      double A[3], B[3], C[3], D[3], CDs[3];
-      shell_geom(ctx, ea, eb, ec, ed, sh.n1, sh.n2, A, B, C, D, CDs);
-      const double za = ctx.pool[ea.z_off + ipa], zb = ctx.pool[eb.z_off + ipb];
-      const double zc = ctx.pool[ec.z_off + ipc], zd = ctx.pool[ed.z_off + ipd];
-      // prepare_Fm (reference src/compute_Fm.cpp:66-159)
-      const double zab = za + zb, inv_zab = 1. / zab, zcd = zc + zd, inv_zcd = 1. / zcd;
-      const double z = zab + zcd, inv_z = 1. / z;
-      double P[3], Q[3], PQs[3], shift[3];
-      for (int q = 0; q < 3; q++) {
-         P[q] = (za * A[q] + zb * B[q]) * inv_zab;
-         Q[q] = (zc * C[q] + zd * D[q]) * inv_zcd;
-      }
-      pbc(Q, P, ctx.cell, PQs);
-      for (int q = 0; q < 3; q++) shift[q] = P[q] - Q[q] - PQs[q];
-      const double normf = 2. * 17.493418327624862 * inv_zab * inv_zcd;   // 2 pi^(5/2) / (zab zcd)
-      double dx = A[0] - B[0], dy = A[1] - B[1], dz = A[2] - B[2];
-      const double RAB2 = dx * dx + dy * dy + dz * dz;
-      const double expon_ab = -(za * zb) / (za + zb) * RAB2;
-      dx = C[0] - D[0]; dy = C[1] - D[1]; dz = C[2] - D[2];
-      const double RCD2 = dx * dx + dy * dy + dz * dz;
-      const double expon_cd = -(zc * zd) / (zc + zd) * RCD2;
-      const double Kfac = (1. / sqrt(z)) * normf * exp(expon_ab + expon_cd);
-      double Cs[3], Ds[3];
-      for (int q = 0; q < 3; q++) {
-         Cs[q] = C[q] + shift[q];
-         Ds[q] = C[q] + CDs[q] + __ldg(ctx.neighs + sh.n2 * 3 + q) + shift[q];
-      }
-      for (int q = 0; q < 3; q++) Q[q] = (zc * Cs[q] + zd * Ds[q]) * inv_zcd;
-      const double rho = zab * zcd * inv_z;
-      const double R = ctx.R_cut * sqrt(rho);
-      const double izab = 1. / zab, i2ab = 0.5 * izab, mrab = -1. * rho * izab * i2ab;
-      const double izcd = 1. / zcd, i2cd = 0.5 * izcd, mrcd = -1. * rho * izcd * i2cd;
-      const double i2z = 0.5 * inv_z;
+      PrimGeo g;
+      prim_geometry(ctx, bt.shells[bt.prm_shell[p]], bt.prm[p], g);
 
       for (int j = lane; j < S; j += TS) acc[j] = 0.0;
       double s00 = 0.0;
@@ -302,12 +352,8 @@ __global__ void __launch_bounds__(256) k_prim(DevCtx ctx, BatchArgs bt, int team
          bool surv = false;
          double *myfm = fmx + lane * (L + 1);
          if (n3 < ctx.Ng) {
-            const double g0 = __ldg(ctx.neighs + n3 * 3 + 0), g1 = __ldg(ctx.neighs + n3 * 3 + 1),
-                         g2 = __ldg(ctx.neighs + n3 * 3 + 2);
-            double PQ0 = P[0] - Q[0] - g0, PQ1 = P[1] - Q[1] - g1, PQ2 = P[2] - Q[2] - g2;
-            double rpq2 = (PQ0 * PQ0 + PQ1 * PQ1 + PQ2 * PQ2);
-            double T = rho * rpq2;
-            const int br = fm_eval(ctx, L, R, T, Kfac, myfm);
+            const double T = image_T(ctx, g, n3);
+            const int br = fm_eval(ctx, L, g.R, T, g.Kfac, myfm);
             c_cheb += (br == 1); c_boys += (br == 2);
             s00 += myfm[0];
             surv = need_vrr && (myfm[0] > 1.e-12);
@@ -321,15 +367,15 @@ __global__ void __launch_bounds__(256) k_prim(DevCtx ctx, BatchArgs bt, int team
                const int n3s = n0 + src;
                const double g0 = __ldg(ctx.neighs + n3s * 3 + 0), g1 = __ldg(ctx.neighs + n3s * 3 + 1),
                             g2 = __ldg(ctx.neighs + n3s * 3 + 2);
-               const double Qp0 = Q[0] + g0, Qp1 = Q[1] + g1, Qp2 = Q[2] + g2;
-               const double W0 = (zab * P[0] + zcd * Qp0) * inv_z;
-               const double W1 = (zab * P[1] + zcd * Qp1) * inv_z;
-               const double W2 = (zab * P[2] + zcd * Qp2) * inv_z;
-               pqz[0] = P[0] - A[0]; pqz[1] = P[1] - A[1]; pqz[2] = P[2] - A[2];
-               pqz[3] = W0 - P[0]; pqz[4] = W1 - P[1]; pqz[5] = W2 - P[2];
-               pqz[6] = Q[0] - Cs[0]; pqz[7] = Q[1] - Cs[1]; pqz[8] = Q[2] - Cs[2];
+               const double Qp0 = g.Q[0] + g0, Qp1 = g.Q[1] + g1, Qp2 = g.Q[2] + g2;
+               const double W0 = (g.zab * g.P[0] + g.zcd * Qp0) * g.inv_z;
+               const double W1 = (g.zab * g.P[1] + g.zcd * Qp1) * g.inv_z;
+               const double W2 = (g.zab * g.P[2] + g.zcd * Qp2) * g.inv_z;
+               pqz[0] = g.PA[0]; pqz[1] = g.PA[1]; pqz[2] = g.PA[2];
+               pqz[3] = W0 - g.P[0]; pqz[4] = W1 - g.P[1]; pqz[5] = W2 - g.P[2];
+               pqz[6] = g.QC[0]; pqz[7] = g.QC[1]; pqz[8] = g.QC[2];
                pqz[9] = W0 - Qp0; pqz[10] = W1 - Qp1; pqz[11] = W2 - Qp2;
-               pqz[12] = i2ab; pqz[13] = mrab; pqz[14] = i2cd; pqz[15] = mrcd; pqz[16] = i2z;
+               pqz[12] = g.i2ab; pqz[13] = g.mrab; pqz[14] = g.i2cd; pqz[15] = g.mrcd; pqz[16] = g.i2z;
                const int n00 = pl->vb[0].nm;
                for (int q = 0; q < n00; q++) ws[q] = myfm[q];
             }
@@ -393,11 +439,6 @@ __global__ void __launch_bounds__(256) k_prim(DevCtx ctx, BatchArgs bt, int team
 // classes, lane-interleaved workspaces) or one image per warp (level-parallel), and the m = 0
 // targets are summed per primitive in shared memory.
 // ---------------------------------------------------------------------------------------
-struct PrimGeo {
-   double P[3], Q[3], PA[3], QC[3];
-   double Kfac, rho, R, zab, zcd, inv_z, i2ab, mrab, i2cd, mrcd, i2z, pad;
-};
-
 template <bool LANE_VRR>
 __global__ void __launch_bounds__(256) k_prim2(DevCtx ctx, BatchArgs bt, int cp, int warp_doubles) {
    extern __shared__ __align__(16) double smem[];
@@ -435,50 +476,8 @@ __global__ void __launch_bounds__(256) k_prim2(DevCtx ctx, BatchArgs bt, int cp,
       // ---- per-primitive geometry (reference src/compute_Fm.cpp:66-159, :202-210, :281-290)
       if (lane < np) {
          const uint32_t p = p0 + lane;
-         const uint32_t code = bt.prm[p];
-         const ShellRec sh = bt.shells[bt.prm_shell[p]];
-         const BasisEnt ea = ctx.ents[sh.ent[0]], eb = ctx.ents[sh.ent[1]];
-         const BasisEnt ec = ctx.ents[sh.ent[2]], ed = ctx.ents[sh.ent[3]];
-         double A[3], B[3], C[3], D[3], CDs[3];
-         shell_geom(ctx, ea, eb, ec, ed, sh.n1, sh.n2, A, B, C, D, CDs);
-         const double za = ctx.pool[ea.z_off + (code >> 24)], zb = ctx.pool[eb.z_off + ((code >> 16) & 255)];
-         const double zc = ctx.pool[ec.z_off + ((code >> 8) & 255)], zd = ctx.pool[ed.z_off + (code & 255)];
-         const double zab = za + zb, inv_zab = 1. / zab, zcd = zc + zd, inv_zcd = 1. / zcd;
-         const double z = zab + zcd, inv_z = 1. / z;
-         double P[3], Q[3], PQs[3], shift[3];
-         for (int q = 0; q < 3; q++) {
-            P[q] = (za * A[q] + zb * B[q]) * inv_zab;
-            Q[q] = (zc * C[q] + zd * D[q]) * inv_zcd;
-         }
-         pbc(Q, P, ctx.cell, PQs);
-         for (int q = 0; q < 3; q++) shift[q] = P[q] - Q[q] - PQs[q];
-         const double normf = 2. * 17.493418327624862 * inv_zab * inv_zcd;
-         double dx = A[0] - B[0], dy = A[1] - B[1], dz = A[2] - B[2];
-         const double RAB2 = dx * dx + dy * dy + dz * dz;
-         const double expon_ab = -(za * zb) / (za + zb) * RAB2;
-         dx = C[0] - D[0]; dy = C[1] - D[1]; dz = C[2] - D[2];
-         const double RCD2 = dx * dx + dy * dy + dz * dz;
-         const double expon_cd = -(zc * zd) / (zc + zd) * RCD2;
          PrimGeo g;
-         g.Kfac = (1. / sqrt(z)) * normf * exp(expon_ab + expon_cd);
-         double Cs[3], Ds[3];
-         for (int q = 0; q < 3; q++) {
-            Cs[q] = C[q] + shift[q];
-            Ds[q] = C[q] + CDs[q] + __ldg(ctx.neighs + sh.n2 * 3 + q) + shift[q];
-         }
-         for (int q = 0; q < 3; q++) {
-            g.P[q] = P[q];
-            g.Q[q] = (zc * Cs[q] + zd * Ds[q]) * inv_zcd;
-            g.PA[q] = P[q] - A[q];
-            g.QC[q] = g.Q[q] - Cs[q];
-         }
-         g.rho = zab * zcd * inv_z;
-         g.R = ctx.R_cut * sqrt(g.rho);
-         g.zab = zab; g.zcd = zcd; g.inv_z = inv_z;
-         const double izab = 1. / zab, izcd = 1. / zcd;
-         g.i2ab = 0.5 * izab; g.mrab = -1. * g.rho * izab * g.i2ab;
-         g.i2cd = 0.5 * izcd; g.mrcd = -1. * g.rho * izcd * g.i2cd;
-         g.i2z = 0.5 * inv_z; g.pad = 0;
+         prim_geometry(ctx, bt.shells[bt.prm_shell[p]], bt.prm[p], g);
          geo[lane] = g;
          s00[lane] = 0.0;
       }
@@ -615,12 +614,8 @@ __global__ void __launch_bounds__(256) k_prim2(DevCtx ctx, BatchArgs bt, int cp,
          if (pi < npair) {
             const int p = pi / Ng, n3 = pi - p * Ng;
             const PrimGeo &g = geo[p];
-            const double PQ0 = g.P[0] - g.Q[0] - __ldg(ctx.neighs + n3 * 3 + 0);
-            const double PQ1 = g.P[1] - g.Q[1] - __ldg(ctx.neighs + n3 * 3 + 1);
-            const double PQ2 = g.P[2] - g.Q[2] - __ldg(ctx.neighs + n3 * 3 + 2);
-            const double rpq2 = (PQ0 * PQ0 + PQ1 * PQ1 + PQ2 * PQ2);
-            T = g.rho * rpq2;
-            pass = !(T > g.R * g.R + 11.0 * g.R + 50.0);
+            T = image_T(ctx, g, n3);
+            pass = !(T > trunc_upper(g.R));
          }
          const unsigned bal = __ballot_sync(0xffffffffu, pass);
          if (pass) {

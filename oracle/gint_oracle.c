@@ -13,7 +13,7 @@
  *   normalisation of contraction coefficients  src/extern_functions.cpp:95-136
  *   add_prm / add_shell / add_qrt / add_qrtt  src/libGint.cpp:151-283
  *   primitive geometry and Kfac               src/compute_Fm.cpp:20-166 (prepare_Fm)
- *   minimum-image wrap                        src/util.cpp:235-265 (compute_pbc)
+ *   minimum-image wrap                        src/util.cpp:132-162 (compute_pbc)
  *   truncated-Coulomb G_m(T,R)                src/t_c_g0_n.cpp:53-180 (fill_x12_to_patch,
  *                                             t_c_g0_n_v2)
  *   Boys function table and evaluation        src/fgamma.cpp:53-123 (fgamma_ref,
@@ -27,7 +27,8 @@
  *   exchange update of K                      src/compute_KS.cpp:6-117
  *
  * Quantities that decide screening (T, R, Kfac, the patch index) are evaluated with the
- * same formula and operation order as the reference. The recursions themselves are written
+ * same formula and operation order as the reference, with one explicit fma where the
+ * reference's CUDA build contracts (wdist below). The recursions themselves are written
  * directly from the Obara-Saika relations (no op-list interpreter); their results agree with
  * the reference's to rounding.
  */
@@ -291,7 +292,7 @@ static int or_tcg(const or_handle *h, double *res, double R, double T, int Nder,
 }
 
 /* ------------------------------------------------------------------------------------ */
-/* periodic wrap (restates src/util.cpp:235-265)                                        */
+/* periodic wrap (restates src/util.cpp:132-162)                                        */
 /* ------------------------------------------------------------------------------------ */
 static void or_pbc(const double A[3], const double B[3], const double *cell, double *AB) {
    const double *hm = &cell[0], *hi = &cell[9];
@@ -305,11 +306,15 @@ static void or_pbc(const double A[3], const double B[3], const double *cell, dou
    AB[2] = hm[0*3+2]*s0 + hm[1*3+2]*s1 + hm[2*3+2]*s2;
 }
 
+/* weighted distance (c1 X1 + c2 X2) c12 (src/util.h:62-68). The reference's CUDA build
+ * contracts the first product into the sum, fma(c1, X1, c2 X2) c12, and that rounding decides
+ * the minimum image of P - Q when it lies on half a lattice vector (symmetric quartets such as
+ * (ab|ab') with b' an image of b and equal exponents), so the oracle states the fma. */
 static void wdist(double X[3], const double X1[3], const double X2[3], double c1, double c2,
                   double c12) {
-   X[0] = (c1*X1[0] + c2*X2[0]) * c12;
-   X[1] = (c1*X1[1] + c2*X2[1]) * c12;
-   X[2] = (c1*X1[2] + c2*X2[2]) * c12;
+   X[0] = fma(c1, X1[0], c2*X2[0]) * c12;
+   X[1] = fma(c1, X1[1], c2*X2[1]) * c12;
+   X[2] = fma(c1, X1[2], c2*X2[2]) * c12;
 }
 
 /* ------------------------------------------------------------------------------------ */

@@ -9,7 +9,7 @@ The fixture pins the CPU oracle and the engine's tables without the reference tr
   c2s          c2s[245]                                         (src/c2s.h:36)
   fg_*         fgamma0(n, T, fac) samples                       (src/fgamma.cpp:196)
   tcg_*        t_c_g0_n_v2 (+fgamma0) samples with a seeded C0  (src/t_c_g0_n.cpp:67)
-  pbc_*        compute_pbc samples                              (src/util.cpp:235)
+  pbc_*        compute_pbc samples                              (src/util.cpp:132)
   plan         pr_size, sh_size, numV, numVC, numVCH of plan(la,lb,lc,ld), l<=3 (src/plan.cpp:217)
 Run: python tests/golden/make_golden.py
 """
