@@ -13,8 +13,13 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "nvcc")
 HOSTCXX = "g++"
 
-ENGINE_SRC = ["engine.cpp", "plan.cpp", "kernels.cu"]
+# (source, extra flags, object name); prim3.cu is compiled once per part so the generated classes
+# compile in parallel
+PRIM3_PARTS = 8
+ENGINE_OBJS = [("engine.cpp", [], "engine.o"), ("plan.cpp", [], "plan.o"), ("kernels.cu", [], "kernels.o")] + \
+    [("prim3.cu", [f"-DPRIM3_PART={i}"], f"prim3_{i}.o") for i in range(PRIM3_PARTS)]
 DRIVER_SRC = ["driver.cpp"]
+OBJDIR = os.path.join(HERE, "_build")
 
 
 def _run(cmd):
@@ -24,25 +29,41 @@ def _run(cmd):
     return r.stdout + r.stderr
 
 
+def _headers():
+    hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    hs.append(os.path.join(HERE, "..", "include", "libgint.h"))
+    return hs
+
+
 def _stale(target, sources):
     if not os.path.exists(target):
         return True
     t = os.path.getmtime(target)
-    deps = list(sources) + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".h")]
-    deps.append(os.path.join(HERE, "..", "include", "libgint.h"))
+    deps = list(sources) + _headers()
     return any(os.path.getmtime(s) > t for s in deps if os.path.exists(s))
 
 
 def build_engine(force=False, verbose=False):
+    """nvcc each translation unit to an object (in parallel), then link the shared library."""
+    from concurrent.futures import ThreadPoolExecutor
     out = os.path.join(LIB, "libgint_b200.so")
-    srcs = [os.path.join(CSRC, f) for f in ENGINE_SRC]
-    if force or _stale(out, srcs):
+    os.makedirs(OBJDIR, exist_ok=True)
+    jobs = []
+    for src, flags, obj in ENGINE_OBJS:
+        s, o = os.path.join(CSRC, src), os.path.join(OBJDIR, obj)
+        if force or _stale(o, [s]):
+            jobs.append([NVCC] + ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
+                                         "-Xptxas", "-v"] + flags + ["-c", s, "-o", o])
+    logs = []
+    if jobs:
+        with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 1)) as ex:
+            logs = list(ex.map(_run, jobs))
+    objs = [os.path.join(OBJDIR, o) for _, _, o in ENGINE_OBJS]
+    if force or jobs or _stale(out, objs):
         os.makedirs(LIB, exist_ok=True)
-        cmd = [NVCC] + ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-                               "-Xptxas", "-v", "-o", out] + srcs + ["-lcudart"]
-        log = _run(cmd)
-        if verbose:
-            print(log)
+        logs.append(_run([NVCC] + ARCH + ["-shared", "-o", out] + objs + ["-lcudart"]))
+    if verbose:
+        print("\n".join(logs))
     return out
 
 

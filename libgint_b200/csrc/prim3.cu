@@ -1,0 +1,296 @@
+// prim3.cu -- k_prim3<la,lb,lc,ld>: Fm + VRR + sum over the third image for the classes whose
+// VRR is generated as straight-line code (vrr_gen.cuh).
+//
+// One warp owns a chunk of CP primitive quartets (reference src/compute_Fm.cpp:20-326,
+// src/compute_VRR.cpp:349-458, src/compute_ECO.cpp:216-272):
+//  1. lane per primitive: the geometry (P, Q, the minimum-image shift, Kfac, R) into shared;
+//  2. lane per (primitive, image) pair: the truncation test T <= R^2 + 11 R + 50; passing
+//     pairs are compacted into a queue;
+//  3. lane per queued pair: G_m (Chebyshev patch series or Boys); pairs with Fm[0] > 1e-12 are
+//     compacted into a second queue; when la = lc = 0 every pair's Fm[0] goes to the (00|00)
+//     target, screened or not, as in the reference;
+//  4. lane per surviving pair: the generated VRR, entirely in registers. Both queues keep the
+//     pairs in primitive order, so pairs of one primitive sit in adjacent lanes; each target is
+//     summed over them by a segmented shuffle reduction and added to the primitive's row of the
+//     warp's shared accumulator by the segment's first lane (no atomics).
+// The chunk's image-summed targets are then stored to AC.
+//
+// Compiled kPrim3Parts times (PRIM3_PART = 0..7); part i instantiates the generated classes
+// whose position in kVrrGenClasses is i modulo kPrim3Parts.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cstdint>
+#include "engine_types.h"
+#include "kernels.h"
+#include "prim3.h"
+#include "prim_common.cuh"
+#include "vrr_gen.cuh"
+
+#ifndef PRIM3_PART
+#define PRIM3_PART 0
+#endif
+
+namespace gint {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+template <int LA, int LB, int LC, int LD>
+struct Prim3Shape {
+   using G = VrrGen<LA, LB, LC, LD>;
+   static constexpr int L = LA + LB + LC + LD, LF = L + 1, S = G::S;
+   // primitives per warp chunk: the largest power of two <= 2048 / S (at most 32), so the shared
+   // accumulator stays near 16 KB per warp
+   static constexpr int CP = S <= 64 ? 32 : (S <= 128 ? 16 : (S <= 256 ? 8 : (S <= 512 ? 4 : (S <= 1024 ? 2 : 1))));
+   static constexpr int PG = (int)(sizeof(PrimGeo) / 8);
+   // per warp, in doubles: geometry, accumulator, queue-1 T, queue-2 Fm, queue indices (2 x 64 ints)
+   static constexpr int WD = CP * PG + CP * S + 64 + 64 * LF + 64;
+};
+
+// Segmented sum over adjacent lanes that carry the same key (keys are contiguous runs); the
+// first lane of each run adds the run's sum to dst[s].
+struct SegSum {
+   unsigned same;   // bit o: lane + 2^o carries this lane's key
+   bool head;
+   double *dst;
+   __device__ __forceinline__ void operator()(int s, double v) {
+#pragma unroll
+      for (int o = 0; o < 5; o++) {
+         const double u = __shfl_down_sync(kFull, v, 1 << o);
+         if (same & (1u << o)) v += u;
+      }
+      if (head) dst[s] += v;
+   }
+};
+
+static __device__ __forceinline__ SegSum make_segsum(int key, int lane, double *dst) {
+   SegSum sg;
+   sg.same = 0;
+#pragma unroll
+   for (int o = 0; o < 5; o++) {
+      const int k2 = __shfl_down_sync(kFull, key, 1 << o);
+      if (lane + (1 << o) < 32 && k2 == key) sg.same |= 1u << o;
+   }
+   const int kp = __shfl_up_sync(kFull, key, 1);
+   sg.head = key >= 0 && (lane == 0 || kp != key);
+   sg.dst = dst;
+   return sg;
+}
+
+template <int LA, int LB, int LC, int LD>
+__global__ void __launch_bounds__(256) k_prim3(DevCtx ctx, BatchArgs bt) {
+   using Sh = Prim3Shape<LA, LB, LC, LD>;
+   using G = typename Sh::G;
+   constexpr int L = Sh::L, LF = Sh::LF, S = Sh::S, CP = Sh::CP;
+   constexpr bool W00 = (LA == 0 && LC == 0);
+   constexpr bool NEED_VRR = G::nout > 0;
+   extern __shared__ __align__(16) double smem[];
+   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+   double *wbase = smem + (size_t)warp * Sh::WD;
+   PrimGeo *geo = reinterpret_cast<PrimGeo *>(wbase);
+   double *acc = wbase + CP * Sh::PG;
+   double *q1t = acc + CP * S;
+   double *q2f = q1t + 64;
+   int *q1i = reinterpret_cast<int *>(q2f + 64 * LF);
+   int *q2i = q1i + 64;
+   const int Ng = ctx.Ng;
+   const unsigned below = (1u << lane) - 1u;
+   unsigned long long c_cheb = 0, c_boys = 0, c_vrr = 0;
+
+   const uint32_t nchunk = (bt.nprm + CP - 1) / CP;
+   for (uint32_t ch = blockIdx.x * nwarp + warp; ch < nchunk; ch += gridDim.x * nwarp) {
+      const uint32_t p0 = ch * CP;
+      const int np = (int)min((uint32_t)CP, bt.nprm - p0);
+      if (lane < np) {
+         PrimGeo g;
+         prim_geometry(ctx, bt.shells[bt.prm_shell[p0 + lane]], bt.prm[p0 + lane], g);
+         geo[lane] = g;
+      }
+      for (int j = lane; j < CP * S; j += 32) acc[j] = 0.0;
+      __syncwarp();
+
+      int n1 = 0, n2 = 0;
+      // stage 4: VRR of queued survivors [0, cnt), one per lane
+      auto run_vrr = [&](int cnt) {
+         const bool act = lane < cnt;
+         const int pi = act ? q2i[lane] : 0;
+         const int p = pi / Ng, n3 = pi - p * Ng;
+         const PrimGeo &g = geo[p];
+         double z[17], F[LF];
+#pragma unroll
+         for (int q = 0; q < 3; q++) {
+            const double Qp = g.Q[q] + __ldg(ctx.neighs + n3 * 3 + q);
+            const double W = (g.zab * g.P[q] + g.zcd * Qp) * g.inv_z;
+            z[q] = g.PA[q];
+            z[3 + q] = W - g.P[q];
+            z[6 + q] = g.QC[q];
+            z[9 + q] = W - Qp;
+         }
+         z[12] = g.i2ab; z[13] = g.mrab; z[14] = g.i2cd; z[15] = g.mrcd; z[16] = g.i2z;
+#pragma unroll
+         for (int m = 0; m < LF; m++) F[m] = act ? q2f[lane * LF + m] : 0.0;
+         SegSum sg = make_segsum(act ? p : -1 - lane, lane, acc + p * S);
+         G::run(F, z, sg);
+         c_vrr += (lane == 0) ? (unsigned)cnt : 0u;
+         __syncwarp();
+      };
+      // stage 3: G_m of queued pairs [0, cnt), one per lane
+      auto run_fm = [&](int cnt) {
+         const bool act = lane < cnt;
+         const int pi = act ? q1i[lane] : 0;
+         const int p = pi / Ng;
+         double fm[LF];
+         bool surv = false;
+         if (act) {
+            const PrimGeo &g = geo[p];
+            const int br = fm_eval_t<L>(ctx, L, g.R, q1t[lane], g.Kfac, fm);
+            c_cheb += (br == 1);
+            c_boys += (br == 2);
+            surv = NEED_VRR && (fm[0] > 1.e-12);
+         } else {
+#pragma unroll
+            for (int m = 0; m < LF; m++) fm[m] = 0.0;
+         }
+         if (W00) {
+            SegSum sg = make_segsum(act ? p : -1 - lane, lane, acc + p * S);
+            sg(G::s00, fm[0]);
+            __syncwarp();
+         }
+         if (NEED_VRR) {
+            const unsigned bal = __ballot_sync(kFull, surv);
+            if (surv) {
+               const int pos = n2 + __popc(bal & below);
+               q2i[pos] = pi;
+#pragma unroll
+               for (int m = 0; m < LF; m++) q2f[pos * LF + m] = fm[m];
+            }
+            n2 += __popc(bal);
+            __syncwarp();
+            if (n2 >= 32) {
+               run_vrr(32);
+               const int rem = n2 - 32;
+               int v = 0;
+               double tmp[LF];
+               if (lane < rem) {
+                  v = q2i[32 + lane];
+#pragma unroll
+                  for (int m = 0; m < LF; m++) tmp[m] = q2f[(32 + lane) * LF + m];
+               }
+               __syncwarp();
+               if (lane < rem) {
+                  q2i[lane] = v;
+#pragma unroll
+                  for (int m = 0; m < LF; m++) q2f[lane * LF + m] = tmp[m];
+               }
+               __syncwarp();
+               n2 = rem;
+            }
+         }
+      };
+      // stage 2: truncation test over every (primitive, image) pair of the chunk
+      const int npair = np * Ng;
+      for (int b0 = 0; b0 < npair; b0 += 32) {
+         const int pi = b0 + lane;
+         bool pass = false;
+         double T = 0.0;
+         if (pi < npair) {
+            const int p = pi / Ng, n3 = pi - p * Ng;
+            const PrimGeo &g = geo[p];
+            T = image_T(ctx, g, n3);
+            pass = !(T > trunc_upper(g.R));
+         }
+         const unsigned bal = __ballot_sync(kFull, pass);
+         if (pass) {
+            const int pos = n1 + __popc(bal & below);
+            q1i[pos] = pi;
+            q1t[pos] = T;
+         }
+         n1 += __popc(bal);
+         __syncwarp();
+         if (n1 >= 32) {
+            run_fm(32);
+            const int rem = n1 - 32;
+            int vi = 0;
+            double vt = 0.0;
+            if (lane < rem) { vi = q1i[32 + lane]; vt = q1t[32 + lane]; }
+            __syncwarp();
+            if (lane < rem) { q1i[lane] = vi; q1t[lane] = vt; }
+            __syncwarp();
+            n1 = rem;
+         }
+      }
+      if (n1 > 0) run_fm(n1);
+      if (NEED_VRR && n2 > 0) run_vrr(n2);
+      __syncwarp();
+      if (lane == 0 && ctx.cnt) atomicAdd(ctx.cnt + bt.cls * 4 + 3, (unsigned long long)np);
+      double *out = bt.AC + (size_t)p0 * S;
+      for (int j = lane; j < np * S; j += 32) out[j] = acc[j];
+      __syncwarp();
+   }
+   if (ctx.cnt) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+         c_cheb += __shfl_down_sync(kFull, c_cheb, o);
+         c_boys += __shfl_down_sync(kFull, c_boys, o);
+      }
+      if (lane == 0) {
+         atomicAdd(ctx.cnt + bt.cls * 4 + 0, c_cheb);
+         atomicAdd(ctx.cnt + bt.cls * 4 + 1, c_boys);
+         atomicAdd(ctx.cnt + bt.cls * 4 + 2, c_vrr);
+      }
+   }
+}
+
+template <int LA, int LB, int LC, int LD>
+cudaError_t launch_one(const DevCtx &ctx, const BatchArgs &bt, cudaStream_t st) {
+   using Sh = Prim3Shape<LA, LB, LC, LD>;
+   const size_t warp_bytes = (size_t)Sh::WD * 8;
+   // about 100 KB per block so that two blocks share an SM
+   const int nw = (int)std::max<size_t>(1, std::min<size_t>(8, (100 * 1024) / warp_bytes));
+   const size_t smem = warp_bytes * nw;
+   cudaError_t e = cudaFuncSetAttribute(k_prim3<LA, LB, LC, LD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem);
+   if (e != cudaSuccess) return e;
+   const long nchunk = ((long)bt.nprm + Sh::CP - 1) / Sh::CP;
+   const long blocks = std::max(1L, std::min((nchunk + nw - 1) / nw, 148L * 16));
+   k_prim3<LA, LB, LC, LD><<<(unsigned)blocks, nw * 32, smem, st>>>(ctx, bt);
+   return cudaGetLastError();
+}
+
+template <int I>
+struct PartTable {
+   static bool launch(int cls, const DevCtx &ctx, const BatchArgs &bt, cudaStream_t st, cudaError_t *err) {
+      if constexpr (I >= kVrrGenCount) {
+         return false;
+      } else {
+         constexpr int c = kVrrGenClasses[I];
+         if (cls == c) {
+            *err = launch_one<(c >> 6) & 3, (c >> 4) & 3, (c >> 2) & 3, c & 3>(ctx, bt, st);
+            return true;
+         }
+         return PartTable<I + kPrim3Parts>::launch(cls, ctx, bt, st, err);
+      }
+   }
+};
+
+}  // namespace
+
+#define PRIM3_CAT2(a, b) a##b
+#define PRIM3_CAT(a, b) PRIM3_CAT2(a, b)
+bool PRIM3_CAT(prim3_launch_part, PRIM3_PART)(const DevCtx &ctx, const BatchArgs &bt, cudaStream_t st,
+                                               cudaError_t *err) {
+   if (bt.nprm == 0) { *err = cudaSuccess; return true; }
+   return PartTable<PRIM3_PART>::launch(bt.cls, ctx, bt, st, err);
+}
+
+#if PRIM3_PART == 0
+bool prim3_launch(const DevCtx &ctx, const BatchArgs &bt, cudaStream_t st, cudaError_t *err) {
+   static_assert(kPrim3Parts == 8, "one call per part below");
+   return prim3_launch_part0(ctx, bt, st, err) || prim3_launch_part1(ctx, bt, st, err) ||
+          prim3_launch_part2(ctx, bt, st, err) || prim3_launch_part3(ctx, bt, st, err) ||
+          prim3_launch_part4(ctx, bt, st, err) || prim3_launch_part5(ctx, bt, st, err) ||
+          prim3_launch_part6(ctx, bt, st, err) || prim3_launch_part7(ctx, bt, st, err);
+}
+#endif
+
+}  // namespace gint

@@ -1,0 +1,26 @@
+// prim3.h -- launcher of k_prim3, the primitive kernel of the classes with generated VRR code.
+#pragma once
+#include <cuda_runtime.h>
+#include "kernels.h"
+
+namespace gint {
+
+// The generated classes are instantiated in kPrim3Parts translation units (prim3.cu compiled
+// with PRIM3_PART = 0..kPrim3Parts-1) so that they compile in parallel.
+constexpr int kPrim3Parts = 8;
+
+// Launches k_prim3 for class bt.cls if that class has generated code; returns false (and
+// launches nothing) otherwise. *err receives the launch status.
+bool prim3_launch(const DevCtx &ctx, const BatchArgs &bt, cudaStream_t st, cudaError_t *err);
+
+// one per part (prim3.cu)
+bool prim3_launch_part0(const DevCtx &ctx, const BatchArgs &bt, cudaStream_t st, cudaError_t *err);
+bool prim3_launch_part1(const DevCtx &ctx, const BatchArgs &bt, cudaStream_t st, cudaError_t *err);
+bool prim3_launch_part2(const DevCtx &ctx, const BatchArgs &bt, cudaStream_t st, cudaError_t *err);
+bool prim3_launch_part3(const DevCtx &ctx, const BatchArgs &bt, cudaStream_t st, cudaError_t *err);
+bool prim3_launch_part4(const DevCtx &ctx, const BatchArgs &bt, cudaStream_t st, cudaError_t *err);
+bool prim3_launch_part5(const DevCtx &ctx, const BatchArgs &bt, cudaStream_t st, cudaError_t *err);
+bool prim3_launch_part6(const DevCtx &ctx, const BatchArgs &bt, cudaStream_t st, cudaError_t *err);
+bool prim3_launch_part7(const DevCtx &ctx, const BatchArgs &bt, cudaStream_t st, cudaError_t *err);
+
+}  // namespace gint
