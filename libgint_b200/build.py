@@ -13,11 +13,13 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "nvcc")
 HOSTCXX = "g++"
 
-# (source, extra flags, object name); prim3.cu is compiled once per part so the generated classes
-# compile in parallel
+# (source, extra flags, object name); prim3.cu and group3.cu are compiled once per part so the
+# generated classes compile in parallel
 PRIM3_PARTS = 8
+GROUP3_PARTS = 4
 ENGINE_OBJS = [("engine.cpp", [], "engine.o"), ("plan.cpp", [], "plan.o"), ("kernels.cu", [], "kernels.o")] + \
-    [("prim3.cu", [f"-DPRIM3_PART={i}"], f"prim3_{i}.o") for i in range(PRIM3_PARTS)]
+    [("prim3.cu", [f"-DPRIM3_PART={i}"], f"prim3_{i}.o") for i in range(PRIM3_PARTS)] + \
+    [("group3.cu", [f"-DGROUP3_PART={i}"], f"group3_{i}.o") for i in range(GROUP3_PARTS)]
 DRIVER_SRC = ["driver.cpp"]
 OBJDIR = os.path.join(HERE, "_build")
 

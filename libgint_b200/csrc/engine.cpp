@@ -364,8 +364,15 @@ static bool upload_tables(Handle *h) {
       h->basis_dirty = false;
    }
    if (h->pot_dirty && h->have_pot) {
-      if (!ensure(h, h->d_C0, h->C0.size() * 8, "C0")) return false;
-      if (!ck(h, cudaMemcpy(h->d_C0.p, h->C0.data(), h->C0.size() * 8, cudaMemcpyHostToDevice), "C0")) return false;
+      // repack to kC0Row doubles per derivative order (32-byte aligned rows, zero padding)
+      const int nord = h->ld_C0 / 105;
+      std::vector<double> packed((size_t)207 * nord * kC0Row, 0.0);
+      for (int p = 0; p < 207; p++)
+         for (int k = 0; k < nord; k++)
+            std::memcpy(&packed[((size_t)p * nord + k) * kC0Row], &h->C0[(size_t)p * h->ld_C0 + (size_t)k * 105],
+                        105 * sizeof(double));
+      if (!ensure(h, h->d_C0, packed.size() * 8, "C0")) return false;
+      if (!ck(h, cudaMemcpy(h->d_C0.p, packed.data(), packed.size() * 8, cudaMemcpyHostToDevice), "C0")) return false;
       h->pot_dirty = false;
    }
    if (h->neighs_dirty) {
@@ -400,7 +407,7 @@ static DevCtx make_ctx(Handle *h) {
    std::memcpy(c.cell, h->cell, sizeof(c.cell));
    c.R_cut = h->R_cut;
    c.C0 = (const double *)h->d_C0.p;
-   c.ld_C0 = h->ld_C0;
+   c.ld_C0 = (h->ld_C0 / 105) * kC0Row;
    c.lut_low = (const uint8_t *)h->d_lut.p;
    c.lut_high = (const uint8_t *)h->d_lut.p + 128 * 128;
    c.bw = (const double *)h->d_bw.p;

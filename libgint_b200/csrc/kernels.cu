@@ -23,6 +23,7 @@
 #include <mutex>
 #include "engine_types.h"
 #include "kernels.h"
+#include "group3.h"
 #include "prim3.h"
 #include "prim_common.cuh"
 
@@ -778,8 +779,20 @@ size_t group_global_scratch(const ClassPlan &hp, int *grid, int *warps) {
    return wd * (size_t)(*warps) * (*grid);
 }
 
+static int g_group_kernel = -1;
+
+// Group-kernel choice: k_group3 (generated HRR, one lane per group) for the classes it covers,
+// then k_group_lane / k_group. LIBGINT_GROUP_KERNEL=2 skips k_group3 (for comparisons).
 cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan &hp, cudaStream_t st) {
    if (bt.ngroup == 0) return cudaSuccess;
+   if (g_group_kernel < 0) {
+      const char *e = getenv("LIBGINT_GROUP_KERNEL");
+      g_group_kernel = (e && e[0] == '2') ? 2 : 3;
+   }
+   if (g_group_kernel == 3) {
+      cudaError_t err = cudaSuccess;
+      if (group3_launch(ctx, bt, st, &err)) return err;
+   }
    const size_t wd = group_warp_doubles(hp);
    if (wd <= 40) {
       // small workspace: one lane per group, 32 groups per warp

@@ -7,6 +7,10 @@
 
 namespace gint {
 
+// Doubles per derivative order in the device copy of C0: 105 coefficients padded to a multiple
+// of four, so that every row starts on a 32-byte boundary.
+constexpr int kC0Row = 108;
+
 // Everything the kernels read besides the batch records (device pointers).
 struct DevCtx {
    const double *pool;        // exponents and normalised coefficients
@@ -16,8 +20,8 @@ struct DevCtx {
    int nspin;
    double cell[18];           // h (rows = lattice vectors) and h^-1
    double R_cut;
-   const double *C0;
-   int ld_C0;
+   const double *C0;          // the caller's Chebyshev table repacked: per patch, (nder+1) rows of
+   int ld_C0;                 // kC0Row doubles (105 coefficients, 3 zeros); ld_C0 = patch stride
    const uint8_t *lut_low, *lut_high;   // 128 x 128 patch maps
    const double *bw;          // per patch: B1, W1, B2, W2
    const double *ftable;      // Boys table, 121 x 28

@@ -39,12 +39,16 @@ template <int LA, int LB, int LC, int LD>
 struct Prim3Shape {
    using G = VrrGen<LA, LB, LC, LD>;
    static constexpr int L = LA + LB + LC + LD, LF = L + 1, S = G::S;
+   static constexpr bool NEED_VRR = G::nout > 0;
    // primitives per warp chunk: the largest power of two <= 2048 / S (at most 32), so the shared
    // accumulator stays near 16 KB per warp
    static constexpr int CP = S <= 64 ? 32 : (S <= 128 ? 16 : (S <= 256 ? 8 : (S <= 512 ? 4 : (S <= 1024 ? 2 : 1))));
    static constexpr int PG = (int)(sizeof(PrimGeo) / 8);
-   // per warp, in doubles: geometry, accumulator, queue-1 T, queue-2 Fm, queue indices (2 x 64 ints)
-   static constexpr int WD = CP * PG + CP * S + 64 + 64 * LF + 64;
+   // per warp, in doubles: geometry, accumulator, queue-1 T and indices, queue-2 Fm and indices
+   static constexpr int WD = CP * PG + CP * S + 64 + 32 + (NEED_VRR ? 64 * LF + 32 : 0);
+   // resident blocks per SM the register budget is sized for (small classes need few registers)
+   static constexpr int MINB = L <= 1 ? 3 : (L <= 3 ? 2 : 1);
+   static constexpr int THREADS = MINB == 3 ? 192 : 256;
 };
 
 // Segmented sum over adjacent lanes that carry the same key (keys are contiguous runs); the
@@ -78,22 +82,30 @@ static __device__ __forceinline__ SegSum make_segsum(int key, int lane, double *
 }
 
 template <int LA, int LB, int LC, int LD>
-__global__ void __launch_bounds__(256) k_prim3(DevCtx ctx, BatchArgs bt) {
+__global__ void __launch_bounds__(Prim3Shape<LA, LB, LC, LD>::THREADS, Prim3Shape<LA, LB, LC, LD>::MINB)
+k_prim3(DevCtx ctx, BatchArgs bt) {
    using Sh = Prim3Shape<LA, LB, LC, LD>;
    using G = typename Sh::G;
    constexpr int L = Sh::L, LF = Sh::LF, S = Sh::S, CP = Sh::CP;
    constexpr bool W00 = (LA == 0 && LC == 0);
-   constexpr bool NEED_VRR = G::nout > 0;
+   constexpr bool NEED_VRR = Sh::NEED_VRR;
    extern __shared__ __align__(16) double smem[];
    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
-   double *wbase = smem + (size_t)warp * Sh::WD;
+   const int Ng = ctx.Ng;
+   // the image vectors, shared by the block
+   double *sneigh = smem;
+   for (int i = threadIdx.x; i < 3 * Ng; i += blockDim.x) sneigh[i] = __ldg(ctx.neighs + i);
+   __syncthreads();
+   double *wbase = smem + ((3 * Ng + 1) & ~1) + (size_t)warp * Sh::WD;
    PrimGeo *geo = reinterpret_cast<PrimGeo *>(wbase);
    double *acc = wbase + CP * Sh::PG;
    double *q1t = acc + CP * S;
-   double *q2f = q1t + 64;
-   int *q1i = reinterpret_cast<int *>(q2f + 64 * LF);
-   int *q2i = q1i + 64;
-   const int Ng = ctx.Ng;
+   int *q1i = reinterpret_cast<int *>(q1t + 64);
+   double *q2f = q1t + 64 + 32;
+   int *q2i = reinterpret_cast<int *>(q2f + 64 * LF);
+   // pair numbering within a chunk: pair = p * Ng + n3; each round of 32 pairs advances a lane
+   // by 32 = adv_p * Ng + adv_n
+   const int adv_p = 32 / Ng, adv_n = 32 - adv_p * Ng;
    const unsigned below = (1u << lane) - 1u;
    unsigned long long c_cheb = 0, c_boys = 0, c_vrr = 0;
 
@@ -113,13 +125,13 @@ __global__ void __launch_bounds__(256) k_prim3(DevCtx ctx, BatchArgs bt) {
       // stage 4: VRR of queued survivors [0, cnt), one per lane
       auto run_vrr = [&](int cnt) {
          const bool act = lane < cnt;
-         const int pi = act ? q2i[lane] : 0;
-         const int p = pi / Ng, n3 = pi - p * Ng;
+         const int pk = act ? q2i[lane] : 0;
+         const int p = pk >> 8, n3 = pk & 255;
          const PrimGeo &g = geo[p];
          double z[17], F[LF];
 #pragma unroll
          for (int q = 0; q < 3; q++) {
-            const double Qp = g.Q[q] + __ldg(ctx.neighs + n3 * 3 + q);
+            const double Qp = g.Q[q] + sneigh[n3 * 3 + q];
             const double W = (g.zab * g.P[q] + g.zcd * Qp) * g.inv_z;
             z[q] = g.PA[q];
             z[3 + q] = W - g.P[q];
@@ -137,13 +149,12 @@ __global__ void __launch_bounds__(256) k_prim3(DevCtx ctx, BatchArgs bt) {
       // stage 3: G_m of queued pairs [0, cnt), one per lane
       auto run_fm = [&](int cnt) {
          const bool act = lane < cnt;
-         const int pi = act ? q1i[lane] : 0;
-         const int p = pi / Ng;
+         const int pk = act ? q1i[lane] : 0;
+         const int p = pk >> 8;
          double fm[LF];
          bool surv = false;
          if (act) {
-            const PrimGeo &g = geo[p];
-            const int br = fm_eval_t<L>(ctx, L, g.R, q1t[lane], g.Kfac, fm);
+            const int br = fm_eval_geo<L>(ctx, L, geo[p], q1t[lane], fm);
             c_cheb += (br == 1);
             c_boys += (br == 2);
             surv = NEED_VRR && (fm[0] > 1.e-12);
@@ -160,7 +171,7 @@ __global__ void __launch_bounds__(256) k_prim3(DevCtx ctx, BatchArgs bt) {
             const unsigned bal = __ballot_sync(kFull, surv);
             if (surv) {
                const int pos = n2 + __popc(bal & below);
-               q2i[pos] = pi;
+               q2i[pos] = pk;
 #pragma unroll
                for (int m = 0; m < LF; m++) q2f[pos * LF + m] = fm[m];
             }
@@ -189,23 +200,28 @@ __global__ void __launch_bounds__(256) k_prim3(DevCtx ctx, BatchArgs bt) {
       };
       // stage 2: truncation test over every (primitive, image) pair of the chunk
       const int npair = np * Ng;
+      int tp = lane / Ng, tn = lane - (lane / Ng) * Ng;
       for (int b0 = 0; b0 < npair; b0 += 32) {
-         const int pi = b0 + lane;
          bool pass = false;
          double T = 0.0;
-         if (pi < npair) {
-            const int p = pi / Ng, n3 = pi - p * Ng;
-            const PrimGeo &g = geo[p];
-            T = image_T(ctx, g, n3);
-            pass = !(T > trunc_upper(g.R));
+         if (b0 + lane < npair) {
+            const PrimGeo &g = geo[tp];
+            const double d0 = rsub(g.D[0], sneigh[tn * 3 + 0]);
+            const double d1 = rsub(g.D[1], sneigh[tn * 3 + 1]);
+            const double d2 = rsub(g.D[2], sneigh[tn * 3 + 2]);
+            T = rmul(g.rho, rdot3(d0, d0, d1, d1, d2, d2));
+            pass = !(T > g.upper);
          }
          const unsigned bal = __ballot_sync(kFull, pass);
          if (pass) {
             const int pos = n1 + __popc(bal & below);
-            q1i[pos] = pi;
+            q1i[pos] = (tp << 8) | tn;
             q1t[pos] = T;
          }
          n1 += __popc(bal);
+         tp += adv_p;
+         tn += adv_n;
+         if (tn >= Ng) { tn -= Ng; tp++; }
          __syncwarp();
          if (n1 >= 32) {
             run_fm(32);
@@ -245,14 +261,17 @@ template <int LA, int LB, int LC, int LD>
 cudaError_t launch_one(const DevCtx &ctx, const BatchArgs &bt, cudaStream_t st) {
    using Sh = Prim3Shape<LA, LB, LC, LD>;
    const size_t warp_bytes = (size_t)Sh::WD * 8;
-   // about 100 KB per block so that two blocks share an SM
-   const int nw = (int)std::max<size_t>(1, std::min<size_t>(8, (100 * 1024) / warp_bytes));
-   const size_t smem = warp_bytes * nw;
+   const size_t neigh_bytes = (size_t)((3 * ctx.Ng + 1) & ~1) * 8;
+   // shared memory per block sized so that MINB blocks share an SM
+   const size_t budget = (220 * 1024) / Sh::MINB;
+   const int maxw = Sh::THREADS / 32;
+   const int nw = (int)std::max<size_t>(1, std::min<size_t>(maxw, (budget - std::min(budget, neigh_bytes)) / warp_bytes));
+   const size_t smem = neigh_bytes + warp_bytes * nw;
    cudaError_t e = cudaFuncSetAttribute(k_prim3<LA, LB, LC, LD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)smem);
    if (e != cudaSuccess) return e;
    const long nchunk = ((long)bt.nprm + Sh::CP - 1) / Sh::CP;
-   const long blocks = std::max(1L, std::min((nchunk + nw - 1) / nw, 148L * 16));
+   const long blocks = std::max(1L, std::min((nchunk + nw - 1) / nw, 148L * 24));
    k_prim3<LA, LB, LC, LD><<<(unsigned)blocks, nw * 32, smem, st>>>(ctx, bt);
    return cudaGetLastError();
 }

@@ -102,9 +102,14 @@ static __device__ __forceinline__ void shell_geom(const DevCtx &ctx, const Basis
 }
 
 // Per-primitive-quartet quantities shared by every image n3.
+// Per-primitive-quartet quantities shared by every image n3. D = P - Q is rounded as the
+// reference's T formula rounds it; upper, lower, X2 and i2 (the truncation bounds and the
+// second patch coordinate, which depend on R only) are evaluated exactly as t_c_g0_n does.
 struct PrimGeo {
-   double P[3], Q[3], PA[3], QC[3];
-   double Kfac, rho, R, zab, zcd, inv_z, i2ab, mrab, i2cd, mrcd, i2z, pad;
+   double P[3], Q[3], PA[3], QC[3], D[3];
+   double Kfac, rho, R, upper, lower, X2;
+   double zab, zcd, inv_z, i2ab, mrab, i2cd, mrcd, i2z;
+   int i2, lowR;
 };
 
 // prepare_Fm and the image-independent part of compute_Vm (reference
@@ -149,20 +154,74 @@ static __device__ __forceinline__ void prim_geometry(const DevCtx &ctx, const Sh
    const double izab = 1. / zab, izcd = 1. / zcd;
    g.i2ab = 0.5 * izab; g.mrab = -1. * g.rho * izab * g.i2ab;
    g.i2cd = 0.5 * izcd; g.mrcd = -1. * g.rho * izcd * g.i2cd;
-   g.i2z = 0.5 * inv_z; g.pad = 0;
+   g.i2z = 0.5 * inv_z;
+   for (int q = 0; q < 3; q++) g.D[q] = rsub(g.P[q], g.Q[q]);
+   // truncation bounds and X2 (reference src/t_c_g0_n.cpp:78-131)
+   g.upper = radd(radd(rmul(g.R, g.R), rmul(11.0, g.R)), 50.0);
+   g.lower = radd(rsub(rmul(g.R, g.R), rmul(11.0, g.R)), 0.0);
+   g.lowR = g.R <= 11.0;
+   g.X2 = g.lowR ? g.R / 11.0 : 11.0 / g.R;
+   int i2 = (int)(g.X2 * 128);
+   g.i2 = i2 == 128 ? 127 : i2;
 }
 
 // T = rho |P - Q - neighs[n3]|^2 (reference src/compute_Fm.cpp:204-210)
 static __device__ __forceinline__ double image_T(const DevCtx &ctx, const PrimGeo &g, int n3) {
-   const double PQ0 = rsub(rsub(g.P[0], g.Q[0]), __ldg(ctx.neighs + n3 * 3 + 0));
-   const double PQ1 = rsub(rsub(g.P[1], g.Q[1]), __ldg(ctx.neighs + n3 * 3 + 1));
-   const double PQ2 = rsub(rsub(g.P[2], g.Q[2]), __ldg(ctx.neighs + n3 * 3 + 2));
+   const double PQ0 = rsub(g.D[0], __ldg(ctx.neighs + n3 * 3 + 0));
+   const double PQ1 = rsub(g.D[1], __ldg(ctx.neighs + n3 * 3 + 1));
+   const double PQ2 = rsub(g.D[2], __ldg(ctx.neighs + n3 * 3 + 2));
    return rmul(g.rho, rdot3(PQ0, PQ0, PQ1, PQ1, PQ2, PQ2));
 }
 
 // the truncation bound R^2 + 11 R + 50 (reference src/t_c_g0_n.cpp:78)
 static __device__ __forceinline__ double trunc_upper(double R) {
    return radd(radd(rmul(R, R), rmul(11.0, R)), 50.0);
+}
+
+// four consecutive doubles from a 32-byte aligned, read-only global address
+static __device__ __forceinline__ void ldg_v4(const double *p, double *v) {
+   asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3]) : "l"(p));
+}
+
+// The degree-13 triangular Chebyshev series of one patch at (X1, X2), orders 0..L, times Kfac
+// (reference src/t_c_g0_n.cpp:133-178).
+template <int LT>
+static __device__ __forceinline__ void cheb_eval(const DevCtx &ctx, int L_rt, int patch, double X1, double X2,
+                                                 double Kfac, double *res) {
+   const int L = LT >= 0 ? LT : L_rt;
+   const double B1 = __ldg(ctx.bw + patch * 4 + 0), W1 = __ldg(ctx.bw + patch * 4 + 1);
+   const double B2 = __ldg(ctx.bw + patch * 4 + 2), W2 = __ldg(ctx.bw + patch * 4 + 3);
+   const double *C0_row = ctx.C0 + (size_t)ctx.ld_C0 * patch;
+   const double SQ2 = 1.4142135623730950488016887242096980785696718753;
+   double TG1 = (2. * X1 - B1) * W1;
+   double TG2 = (2. * X2 - B2) * W2;
+   double T1[14], T2[14];
+   T1[0] = 1.0; T2[0] = 1.0;
+   T1[1] = SQ2 * TG1; T2[1] = SQ2 * TG2;
+   T1[2] = 2. * TG1 * T1[1] - SQ2; T2[2] = 2. * TG2 * T2[1] - SQ2;
+#pragma unroll
+   for (int i = 3; i < 14; i++) {
+      T1[i] = 2. * TG1 * T1[i - 1] - T1[i - 2];
+      T2[i] = 2. * TG2 * T2[i - 1] - T2[i - 2];
+   }
+   for (int k = 0; k <= L; k++) {
+      // one 32-byte load per four coefficients (each lane reads its own patch, so a narrower
+      // load would fetch every sector four times)
+      const double *c = C0_row + k * kC0Row;
+      double cf[kC0Row];
+#pragma unroll
+      for (int q = 0; q < kC0Row / 4; q++) ldg_v4(c + 4 * q, cf + 4 * q);
+      double tmp = 0.0;
+      int jl = 0;
+#pragma unroll
+      for (int j = 0; j < 14; j++) {
+         double dot = 0.0;
+#pragma unroll
+         for (int l = 0; l < 14 - j; l++) { dot += T1[l] * cf[jl]; jl++; }
+         tmp += dot * T2[j];
+      }
+      res[k] = tmp * Kfac;
+   }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -203,39 +262,43 @@ static __device__ __forceinline__ int fm_eval_t(const DevCtx &ctx, int L_rt, dou
       if (i2 == 128) i2 = 127;
       patch = __ldg(ctx.lut_high + i1 * 128 + i2);
    }
-   const double B1 = __ldg(ctx.bw + patch * 4 + 0), W1 = __ldg(ctx.bw + patch * 4 + 1);
-   const double B2 = __ldg(ctx.bw + patch * 4 + 2), W2 = __ldg(ctx.bw + patch * 4 + 3);
-   const double *C0_row = ctx.C0 + (size_t)ctx.ld_C0 * patch;
-   const double SQ2 = 1.4142135623730950488016887242096980785696718753;
-   double TG1 = (2. * X1 - B1) * W1;
-   double TG2 = (2. * X2 - B2) * W2;
-   double T1[14], T2[14];
-   T1[0] = 1.0; T2[0] = 1.0;
-   T1[1] = SQ2 * TG1; T2[1] = SQ2 * TG2;
-   T1[2] = 2. * TG1 * T1[1] - SQ2; T2[2] = 2. * TG2 * T2[1] - SQ2;
-#pragma unroll
-   for (int i = 3; i < 14; i++) {
-      T1[i] = 2. * TG1 * T1[i - 1] - T1[i - 2];
-      T2[i] = 2. * TG2 * T2[i - 1] - T2[i - 2];
-   }
-   for (int k = 0; k <= L; k++) {
-      const double *c = C0_row + k * 105;
-      double tmp = 0.0;
-      int jl = 0;
-#pragma unroll
-      for (int j = 0; j < 14; j++) {
-         double dot = 0.0;
-#pragma unroll
-         for (int l = 0; l < 14 - j; l++) { dot += T1[l] * __ldg(c + jl); jl++; }
-         tmp += dot * T2[j];
-      }
-      res[k] = tmp * Kfac;
-   }
+   cheb_eval<LT>(ctx, L, patch, X1, X2, Kfac, res);
    return 1;
 }
 
 static __device__ int fm_eval(const DevCtx &ctx, int L, double R, double T, double Kfac, double *res) {
    return fm_eval_t<-1>(ctx, L, R, T, Kfac, res);
+}
+
+// G_m * Kfac of one image from the primitive's precomputed bounds and X2; the same decisions and
+// arithmetic as fm_eval_t. Returns 0 beyond the truncation, 1 for the series, 2 for Boys.
+template <int LT>
+static __device__ __forceinline__ int fm_eval_geo(const DevCtx &ctx, int L_rt, const PrimGeo &g, double T,
+                                                  double *res) {
+   const int L = LT >= 0 ? LT : L_rt;
+   if (T > g.upper) {
+      for (int n = 0; n <= L; n++) res[n] = 0.0;
+      return 0;
+   }
+   double X1;
+   int patch;
+   if (g.lowR) {
+      X1 = rsub(T, 0.0) / rsub(g.upper, 0.0);
+      int i1 = (int)(X1 * 128);
+      if (i1 == 128) i1 = 127;
+      patch = __ldg(ctx.lut_low + i1 * 128 + g.i2);
+   } else {
+      if (T < g.lower) {
+         boys_eval_t<LT>(L, T, res, ctx.ftable, g.Kfac);
+         return 2;
+      }
+      X1 = rsub(T, g.lower) / rsub(g.upper, g.lower);
+      int i1 = (int)(X1 * 128);
+      if (i1 == 128) i1 = 127;
+      patch = __ldg(ctx.lut_high + i1 * 128 + g.i2);
+   }
+   cheb_eval<LT>(ctx, L, patch, X1, g.X2, g.Kfac, res);
+   return 1;
 }
 
 }  // namespace gint
