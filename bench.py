@@ -6,7 +6,9 @@ One step = one K build over the whole screened quartet list of the workload:
          K recomputed from it (libgint_replay: zero K, all kernels), timed with CUDA events on
          the engine's stream; shell quartets per second over all ranks.
   e2e    the same metric through the C-ABI as a caller uses it: libgint_set_P from host memory,
-         the full add_* call stream, libgint_get_K back to host memory.
+         the full add_* call stream, libgint_get_K back to host memory, from --host-threads
+         caller threads with one handle each (the reference's one handle per OpenMP thread);
+         the threads' K are summed on the host inside the timed region.
 The reference arm (--impl reference) times the CPU restatement of the path (the oracle) on
 the host cores over a strided sample of the same workload.
 
@@ -45,6 +47,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--host-threads", type=int, default=min(8, os.cpu_count() or 1),
+                    help="caller threads (one handle each) of the end-to-end leg")
     return ap.parse_args()
 
 
@@ -273,26 +277,40 @@ def run_ours(args, world, rank, local):
             if line.startswith("bytes_per_launch:"):
                 traffic = float(line.split(":")[1])
 
-    # 4) e2e through the C-ABI with host buffers: set_P, add_* stream, get_K
-    for _ in range(max(0, args.warmup - 1)):
-        sess.build_K_subset(idx)
+    # 4) e2e through the C-ABI with host buffers: set_P, add_* stream, get_K, driven as a caller
+    #    with one handle per host thread does (each thread streams a contiguous share of this
+    #    rank's set quartets; the threads' K are summed on the host)
+    from libgint_b200.workload import MultiSession
+    msess = MultiSession(api, wl, args.host_threads)
+
+    def h2d_total():
+        tot = 0
+        for hh in msess.hs:
+            lib.libgint_get_stats(ctypes.c_void_p(hh), stats)
+            tot += int(stats[5])
+        return tot
+
+    for _ in range(max(1, args.warmup - 1)):
+        msess.build_K(idx=idx)
     barrier()
-    lib.libgint_get_stats(h, stats)
-    h2d0 = stats[5]
+    h2d0 = h2d_total()
     e2e_ms = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        K, _, _ = sess.build_K_subset(idx)
+        K, _, _ = msess.build_K(idx=idx)
         K = sum_K(K)
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
     barrier()
-    check()
-    lib.libgint_get_stats(h, stats)
-    h2d = (stats[5] - h2d0) // max(1, args.steps)
+    for hh in msess.hs:
+        e = lib.libgint_last_error(ctypes.c_void_p(hh))
+        if e:
+            raise RuntimeError(f"engine error {e}: {lib.libgint_error_string(ctypes.c_void_p(hh)).decode()}")
+    h2d = (h2d_total() - h2d0) // max(1, args.steps)
+    msess.close()
     e2e_tot = max_over_ranks(float(np.sum(e2e_ms)))
     e2e_ms_step = e2e_tot / args.steps
     e2e_value = total_shells / (e2e_ms_step / 1e3)
-    d2h = wl.info["flat_size"] * 8
+    d2h = wl.info["flat_size"] * 8 * args.host_threads
     ex = wl.exchange_energy(K)
 
     # 5) CPU baseline (rank 0 at N=1): the oracle on a strided sample, plus parity on it
@@ -319,7 +337,8 @@ def run_ours(args, world, rank, local):
             "ms_per_scf_iter": e2e_ms_step,
             "E_x": ex,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms_step},
+                    "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms_step,
+                    "host_threads": args.host_threads},
             "gpu_launches": int(launches),
             "roofline": {"bound": "fp64", "kernel": "k_prim (Fm + VRR + image sum)",
                          "achieved": prim_tflops, "peak": peak, "unit": "TFLOP/s",

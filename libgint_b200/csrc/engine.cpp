@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -216,9 +217,17 @@ struct Slot {
    bool busy = false, copy_busy = false;
 };
 
+// Class segments of one batch are independent (K is updated with atomics), so they run on
+// kWorkStreams worker streams that fork from and join back to the handle's stream; the tails of
+// one class's kernels then overlap the next class's.
+constexpr int kWorkStreams = 4;
+
 struct Handle {
    int device = 0;
    cudaStream_t stream = nullptr;
+   cudaStream_t work[kWorkStreams] = {};
+   cudaEvent_t work_ev[kWorkStreams] = {};
+   cudaEvent_t fork_ev = nullptr;
    int err = 0;
    std::string errmsg;
    // potential and tables
@@ -314,12 +323,27 @@ static inline OpenGroup *open_group(Handle *h, int c) {
 
 static void ensure_ent_base(Handle *h);
 
+// makes the handle's device current on the calling thread (a caller thread may never have
+// touched CUDA, or may drive handles of several devices)
+static void use_device(Handle *h) {
+   int d = -1;
+   if (cudaGetDevice(&d) != cudaSuccess || d != h->device) ck(h, cudaSetDevice(h->device), "cudaSetDevice");
+}
+
+// host -> device copy on the handle's stream; callers synchronise the stream before returning
+// when the source may be released (the handle's streams do not order against the legacy stream)
+static bool h2d(Handle *h, void *dst, const void *src, size_t bytes, const char *what) {
+   return ck(h, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->stream), what);
+}
+
 static bool upload_tables(Handle *h) {
    if (h->err) return false;
+   use_device(h);
    ensure_ent_base(h);
+   bool uploaded = false;
    if (!h->plans_ready) {
       if (!ensure(h, h->d_plans, sizeof(ClassPlan) * 256, "plans")) return false;
-      if (!ck(h, cudaMemcpy(h->d_plans.p, h->plans, sizeof(ClassPlan) * 256, cudaMemcpyHostToDevice), "plans")) return false;
+      if (!h2d(h, h->d_plans.p, h->plans, sizeof(ClassPlan) * 256, "plans")) return false;
       std::vector<uint8_t> lut;
       std::vector<double> bw;
       make_patch_tables(lut, bw);
@@ -328,15 +352,16 @@ static bool upload_tables(Handle *h) {
       if (!ensure(h, h->d_lut, lut.size(), "lut") || !ensure(h, h->d_bw, bw.size() * 8, "bw") ||
           !ensure(h, h->d_ft, ft.size() * 8, "ftable") || !ensure(h, h->d_err, sizeof(int) * 4, "err"))
          return false;
-      if (!ck(h, cudaMemcpy(h->d_lut.p, lut.data(), lut.size(), cudaMemcpyHostToDevice), "lut")) return false;
-      if (!ck(h, cudaMemcpy(h->d_bw.p, bw.data(), bw.size() * 8, cudaMemcpyHostToDevice), "bw")) return false;
-      if (!ck(h, cudaMemcpy(h->d_ft.p, ft.data(), ft.size() * 8, cudaMemcpyHostToDevice), "ftable")) return false;
+      if (!h2d(h, h->d_lut.p, lut.data(), lut.size(), "lut")) return false;
+      if (!h2d(h, h->d_bw.p, bw.data(), bw.size() * 8, "bw")) return false;
+      if (!h2d(h, h->d_ft.p, ft.data(), ft.size() * 8, "ftable")) return false;
       if (!ck(h, cudaMemset(h->d_err.p, 0, sizeof(int) * 4), "err")) return false;
       double c2s[4][70];
       make_c2s(c2s);
       const double symm[5] = {2.0, 1.0, 0.5, 0.25, 0.0};
       if (!ck(h, upload_constant_tables(&c2s[0][0], symm), "constant tables")) return false;
       h->plans_ready = true;
+      uploaded = true;
    }
    if (h->basis_dirty) {
       std::vector<double> pool;
@@ -359,9 +384,10 @@ static bool upload_tables(Handle *h) {
       if (ents.empty()) ents.push_back(BasisEnt{});
       if (!ensure(h, h->d_pool, pool.size() * 8, "basis") || !ensure(h, h->d_ents, ents.size() * sizeof(BasisEnt), "basis"))
          return false;
-      if (!ck(h, cudaMemcpy(h->d_pool.p, pool.data(), pool.size() * 8, cudaMemcpyHostToDevice), "basis")) return false;
-      if (!ck(h, cudaMemcpy(h->d_ents.p, ents.data(), ents.size() * sizeof(BasisEnt), cudaMemcpyHostToDevice), "basis")) return false;
+      if (!h2d(h, h->d_pool.p, pool.data(), pool.size() * 8, "basis")) return false;
+      if (!h2d(h, h->d_ents.p, ents.data(), ents.size() * sizeof(BasisEnt), "basis")) return false;
       h->basis_dirty = false;
+      uploaded = true;
    }
    if (h->pot_dirty && h->have_pot) {
       // repack to kC0Row doubles per derivative order (32-byte aligned rows, zero padding)
@@ -372,14 +398,18 @@ static bool upload_tables(Handle *h) {
             std::memcpy(&packed[((size_t)p * nord + k) * kC0Row], &h->C0[(size_t)p * h->ld_C0 + (size_t)k * 105],
                         105 * sizeof(double));
       if (!ensure(h, h->d_C0, packed.size() * 8, "C0")) return false;
-      if (!ck(h, cudaMemcpy(h->d_C0.p, packed.data(), packed.size() * 8, cudaMemcpyHostToDevice), "C0")) return false;
+      if (!h2d(h, h->d_C0.p, packed.data(), packed.size() * 8, "C0")) return false;
       h->pot_dirty = false;
+      uploaded = true;
    }
    if (h->neighs_dirty) {
       if (!ensure(h, h->d_neighs, h->neighs.size() * 8, "neighs")) return false;
-      if (!ck(h, cudaMemcpy(h->d_neighs.p, h->neighs.data(), h->neighs.size() * 8, cudaMemcpyHostToDevice), "neighs")) return false;
+      if (!h2d(h, h->d_neighs.p, h->neighs.data(), h->neighs.size() * 8, "neighs")) return false;
       h->neighs_dirty = false;
+      uploaded = true;
    }
+   // the sources above are temporaries or may change: wait for the copies
+   if (uploaded && !ck(h, cudaStreamSynchronize(h->stream), "table upload")) return false;
    return true;
 }
 
@@ -394,6 +424,26 @@ static void ensure_ent_base(Handle *h) {
       n += h->sets[s].nL;
    }
    h->ent_dirty = false;
+}
+
+// worker streams wait for everything queued so far on the handle's stream
+static void fork_workers(Handle *h) {
+   ck(h, cudaEventRecord(h->fork_ev, h->stream), "event record");
+   for (int w = 0; w < kWorkStreams; w++) ck(h, cudaStreamWaitEvent(h->work[w], h->fork_ev, 0), "stream wait");
+}
+
+// the handle's stream waits for everything queued on the worker streams
+static void join_workers(Handle *h) {
+   for (int w = 0; w < kWorkStreams; w++) {
+      ck(h, cudaEventRecord(h->work_ev[w], h->work[w]), "event record");
+      ck(h, cudaStreamWaitEvent(h->stream, h->work_ev[w], 0), "stream wait");
+   }
+}
+
+// The worker stream of the i-th segment of a batch. Segments whose group kernel uses the shared
+// global HRR scratch all go to worker 0, so they never run concurrently.
+static cudaStream_t worker_for(Handle *h, int i, bool uses_scratch) {
+   return uses_scratch ? h->work[0] : h->work[1 + i % (kWorkStreams - 1)];
 }
 
 static DevCtx make_ctx(Handle *h) {
@@ -439,6 +489,7 @@ static void clear_queues(Handle *h) {
 
 static void flush(Handle *h) {
    if (h->active.empty()) return;
+   use_device(h);
    if (h->err) { clear_queues(h); return; }   // drop queued work after an error
    if (!upload_tables(h)) { clear_queues(h); return; }
    if (h->nspin == 0 || !h->d_K[0].p) { set_error(h, 4, "work queued before libgint_set_P"); clear_queues(h); return; }
@@ -495,6 +546,8 @@ static void flush(Handle *h) {
    ck(h, cudaEventRecord(s.ev_copy, h->stream), "event record");
    s.copy_busy = true;
    DevCtx ctx = make_ctx(h);
+   fork_workers(h);
+   int nseg = 0;
    for (const Seg &g : segs) {
       ClassQ &Q = h->q[g.c];
       const ClassPlan &hp = h->plans[g.c];
@@ -518,12 +571,14 @@ static void flush(Handle *h) {
          if (!ensure(h, s.gscr, gs * 8, "HRR scratch")) return;
          bt.gscratch = (double *)s.gscr.p;
       }
-      if (!ck(h, launch_prim(ctx, bt, hp, h->stream), "k_prim launch")) return;
-      if (!ck(h, launch_group(ctx, bt, hp, h->stream), "k_group launch")) return;
+      cudaStream_t ws = worker_for(h, nseg++, gs != 0);
+      if (!ck(h, launch_prim(ctx, bt, hp, ws), "k_prim launch")) return;
+      if (!ck(h, launch_group(ctx, bt, hp, ws), "k_group launch")) return;
       h->n_launch += 2;
       if (rb) rb->segs.push_back({g.c, g.o_prm, g.o_ps, g.o_sh, g.o_g, g.o_q, g.ac_off, bt.nprm, bt.nshell, bt.ngroup});
       h->n_prims += bt.nprm; h->n_shells += bt.nshell; h->n_groups += bt.ngroup;
    }
+   join_workers(h);
    ck(h, cudaEventRecord(s.ev, h->stream), "event record");
    s.busy = true;
    h->n_flush++;
@@ -554,6 +609,7 @@ static void drain(Handle *h) {
 }
 
 static void set_P_impl(Handle *h, int nspin, const double *Pa, const double *Pb, int n) {
+   use_device(h);
    if (n <= 0) { set_error(h, 2, "P_size must be positive"); return; }
    // the previous build must be complete before P/K are replaced
    for (Slot &s : h->slots) if (s.busy) { ck(h, cudaEventSynchronize(s.ev), "slot wait"); s.busy = false; }
@@ -564,14 +620,17 @@ static void set_P_impl(Handle *h, int nspin, const double *Pa, const double *Pb,
    const double *src[2] = {Pa, Pb};
    for (int sp = 0; sp < nspin; sp++) {
       if (!ensure(h, h->d_P[sp], (size_t)n * 8, "P") || !ensure(h, h->d_K[sp], (size_t)n * 8, "K")) return;
-      if (!ck(h, cudaMemcpy(h->d_P[sp].p, src[sp], (size_t)n * 8, cudaMemcpyHostToDevice), "P upload")) return;
+      if (!h2d(h, h->d_P[sp].p, src[sp], (size_t)n * 8, "P upload")) return;
       h->h2d_bytes += (long long)n * 8;
       if (!ck(h, cudaMemsetAsync(h->d_K[sp].p, 0, (size_t)n * 8, h->stream), "K zero")) return;
    }
+   // P is copied at call time (the caller may reuse its array)
+   if (!ck(h, cudaStreamSynchronize(h->stream), "P upload")) return;
    upload_tables(h);
 }
 
 static void get_K_impl(Handle *h, double *Ka, double *Kb) {
+   use_device(h);
    drain(h);
    if (h->nspin == 0) { set_error(h, 4, "libgint_get_K before libgint_set_P"); return; }
    double *dst[2] = {Ka, Kb};
@@ -583,6 +642,7 @@ static void get_K_impl(Handle *h, double *Ka, double *Kb) {
 // milliseconds measured with CUDA events on the handle's stream.
 static double replay_impl(Handle *h, double *kt, double *kcls = nullptr) {
    if (h->err) return -1.0;
+   use_device(h);
    if (h->recs.empty()) { set_error(h, 4, "libgint_replay: nothing recorded"); return -1.0; }
    if (!upload_tables(h)) return -1.0;
    size_t ac = 0, gs = 0;
@@ -604,6 +664,11 @@ static double replay_impl(Handle *h, double *kt, double *kcls = nullptr) {
       if (!kt) return;
       cudaEvent_t e; cudaEventCreate(&e); cudaEventRecord(e, h->stream); kev.push_back(e);
    };
+   // per-kernel timing needs the launches in order on one stream; otherwise the segments spread
+   // over the worker streams
+   const bool spread = kt == nullptr;
+   if (spread) fork_workers(h);
+   int nseg = 0;
    for (auto &rb : h->recs) {
       char *base = (char *)rb.rec.p;
       for (auto &g : rb.segs) {
@@ -619,15 +684,19 @@ static double replay_impl(Handle *h, double *kt, double *kcls = nullptr) {
          bt.nprm = g.nprm; bt.nshell = g.nshell; bt.ngroup = g.ngroup;
          bt.AC = (double *)h->rec_ac.p + g.ac_off;
          bt.gscratch = (double *)h->rec_gscr.p;
+         int a_, b_;
+         cudaStream_t st = spread ? worker_for(h, nseg++, group_global_scratch(h->plans[g.c], &a_, &b_) != 0)
+                                  : h->stream;
          kmark();
          if (kt) kcl.push_back(g.c);
-         if (!ck(h, launch_prim(ctx, bt, h->plans[g.c], h->stream), "k_prim launch")) break;
+         if (!ck(h, launch_prim(ctx, bt, h->plans[g.c], st), "k_prim launch")) break;
          kmark();
-         if (!ck(h, launch_group(ctx, bt, h->plans[g.c], h->stream), "k_group launch")) break;
+         if (!ck(h, launch_group(ctx, bt, h->plans[g.c], st), "k_group launch")) break;
          kmark();
          h->n_launch += 2;
       }
    }
+   if (spread) join_workers(h);
    ck(h, cudaEventRecord(e1, h->stream), "event");
    ck(h, cudaEventSynchronize(e1), "replay");
    if (kt) {
@@ -668,7 +737,19 @@ void *libgint_create_handle(void) {
 void libgint_init(void *hh) {
    Handle *h = (Handle *)hh;
    ck(h, cudaGetDevice(&h->device), "cudaGetDevice");
+   // every kernel loaded once per device before any handle launches (see preload_kernels)
+   static std::once_flag loaded[kMaxDevices];
+   if (h->device >= 0 && h->device < kMaxDevices) {
+      cudaError_t pe = cudaSuccess;
+      std::call_once(loaded[h->device], [&]() { pe = preload_kernels(); });
+      ck(h, pe, "kernel preload");
+   }
    if (!h->stream) ck(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream");
+   for (int w = 0; w < kWorkStreams; w++) {
+      if (!h->work[w]) ck(h, cudaStreamCreateWithFlags(&h->work[w], cudaStreamNonBlocking), "stream");
+      if (!h->work_ev[w]) ck(h, cudaEventCreateWithFlags(&h->work_ev[w], cudaEventDisableTiming), "event");
+   }
+   if (!h->fork_ev) ck(h, cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming), "event");
    for (Slot &s : h->slots) {
       if (!s.ev) ck(h, cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming), "event");
       if (!s.ev_copy) ck(h, cudaEventCreateWithFlags(&s.ev_copy, cudaEventDisableTiming), "event");
@@ -703,15 +784,17 @@ void libgint_set_K(void *hh, double *K, int K_size) {
    Handle *h = (Handle *)hh;
    if (h->nspin < 1 || (size_t)K_size != h->FP_size) { set_error(h, 2, "libgint_set_K: call set_P first with the same size"); return; }
    drain(h);
-   ck(h, cudaMemcpy(h->d_K[0].p, K, (size_t)K_size * 8, cudaMemcpyHostToDevice), "K upload");
+   h2d(h, h->d_K[0].p, K, (size_t)K_size * 8, "K upload");
+   ck(h, cudaStreamSynchronize(h->stream), "K upload");
 }
 
 void libgint_set_K_polarized(void *hh, double *Ka, double *Kb, int K_size) {
    Handle *h = (Handle *)hh;
    if (h->nspin < 2 || (size_t)K_size != h->FP_size) { set_error(h, 2, "libgint_set_K_polarized: call set_P_polarized first"); return; }
    drain(h);
-   ck(h, cudaMemcpy(h->d_K[0].p, Ka, (size_t)K_size * 8, cudaMemcpyHostToDevice), "K upload");
-   ck(h, cudaMemcpy(h->d_K[1].p, Kb, (size_t)K_size * 8, cudaMemcpyHostToDevice), "K upload");
+   h2d(h, h->d_K[0].p, Ka, (size_t)K_size * 8, "K upload");
+   h2d(h, h->d_K[1].p, Kb, (size_t)K_size * 8, "K upload");
+   ck(h, cudaStreamSynchronize(h->stream), "K upload");
 }
 
 void libgint_get_K(void *hh, double *K) { get_K_impl((Handle *)hh, K, nullptr); }
@@ -1144,6 +1227,11 @@ void libgint_destroy_handle(void *hh) {
    DBuf *bufs[] = {&h->d_pool, &h->d_ents, &h->d_neighs, &h->d_C0, &h->d_lut, &h->d_bw, &h->d_ft,
                    &h->d_plans, &h->d_err, &h->d_P[0], &h->d_P[1], &h->d_K[0], &h->d_K[1]};
    for (DBuf *b : bufs) release(*b);
+   for (int w = 0; w < kWorkStreams; w++) {
+      if (h->work[w]) cudaStreamDestroy(h->work[w]);
+      if (h->work_ev[w]) cudaEventDestroy(h->work_ev[w]);
+   }
+   if (h->fork_ev) cudaEventDestroy(h->fork_ev);
    if (h->stream) cudaStreamDestroy(h->stream);
    delete h;
 }

@@ -127,6 +127,22 @@ struct PartTable {
    }
 };
 
+// loads (and so registers with the runtime) every kernel of this part
+template <int I>
+struct PartPreload {
+   static cudaError_t run() {
+      if constexpr (I >= kGrpGenCount) {
+         return cudaSuccess;
+      } else {
+         constexpr int c = kGrpGenClasses[I];
+         cudaFuncAttributes a;
+         cudaError_t e = cudaFuncGetAttributes(&a, k_group3<(c >> 6) & 3, (c >> 4) & 3, (c >> 2) & 3, c & 3>);
+         if (e != cudaSuccess) return e;
+         return PartPreload<I + kGroup3Parts>::run();
+      }
+   }
+};
+
 }  // namespace
 
 #define GROUP3_CAT2(a, b) a##b
@@ -137,7 +153,19 @@ bool GROUP3_CAT(group3_launch_part, GROUP3_PART)(const DevCtx &ctx, const BatchA
    return PartTable<GROUP3_PART>::launch(bt.cls, ctx, bt, st, err);
 }
 
+cudaError_t GROUP3_CAT(group3_preload_part, GROUP3_PART)() { return PartPreload<GROUP3_PART>::run(); }
+
 #if GROUP3_PART == 0
+cudaError_t group3_preload() {
+   cudaError_t (*parts[])() = {group3_preload_part0, group3_preload_part1, group3_preload_part2,
+                               group3_preload_part3};
+   for (auto f : parts) {
+      cudaError_t e = f();
+      if (e != cudaSuccess) return e;
+   }
+   return cudaSuccess;
+}
+
 bool group3_launch(const DevCtx &ctx, const BatchArgs &bt, cudaStream_t st, cudaError_t *err) {
    static_assert(kGroup3Parts == 4, "one call per part below");
    return group3_launch_part0(ctx, bt, st, err) || group3_launch_part1(ctx, bt, st, err) ||

@@ -689,7 +689,6 @@ static cudaError_t launch_prim_t(const DevCtx &ctx, const BatchArgs &bt, const C
    teams = std::min(teams, 256 / TS);
    if (teams < 1) return cudaErrorInvalidConfiguration;
    const size_t smem = plan_bytes + (size_t)teams * team_doubles * 8;
-   cudaFuncSetAttribute(k_prim<TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
    long blocks = ((long)bt.nprm + teams - 1) / teams;
    blocks = std::max(1L, std::min(blocks, 148L * 64));
    k_prim<TS><<<(unsigned)blocks, teams * TS, smem, st>>>(ctx, bt, team_doubles);
@@ -745,10 +744,8 @@ cudaError_t launch_prim(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan 
          const long nchunk = ((long)bt.nprm + cp - 1) / cp;
          long blocks = std::max(1L, std::min((nchunk + nw - 1) / nw, 148L * 32));
          if (lane) {
-            cudaFuncSetAttribute(k_prim2<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             k_prim2<true><<<(unsigned)blocks, nw * 32, smem, st>>>(ctx, bt, cp, (int)wd);
          } else {
-            cudaFuncSetAttribute(k_prim2<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             k_prim2<false><<<(unsigned)blocks, nw * 32, smem, st>>>(ctx, bt, cp, (int)wd);
          }
          return cudaGetLastError();
@@ -800,7 +797,6 @@ cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan
       const size_t plan_bytes = (size_t)plan_smem_doubles() * 8;
       const int nw = 8;
       const size_t smem = plan_bytes + (size_t)nw * 32 * lane_doubles * 8;
-      cudaFuncSetAttribute(k_group_lane, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       long blocks = ((long)bt.ngroup + nw * 32 - 1) / (nw * 32);
       blocks = std::max(1L, std::min(blocks, 148L * 16));
       k_group_lane<<<(unsigned)blocks, nw * 32, smem, st>>>(ctx, bt, lane_doubles);
@@ -812,14 +808,12 @@ cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan
    if (nw >= 1) {
       nw = std::min(nw, 8);
       const size_t smem = plan_bytes + (size_t)nw * wd * 8;
-      cudaFuncSetAttribute(k_group, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       long blocks = ((long)bt.ngroup + nw - 1) / nw;
       blocks = std::max(1L, std::min(blocks, 148L * 64));
       k_group<<<(unsigned)blocks, nw * 32, smem, st>>>(ctx, bt, (int)wd, 0);
    } else {
       int grid = 0, warps = 0;
       group_global_scratch(hp, &grid, &warps);
-      cudaFuncSetAttribute(k_group, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan_bytes);
       k_group<<<grid, warps * 32, plan_bytes, st>>>(ctx, bt, (int)wd, 1);
    }
    return cudaGetLastError();
@@ -863,6 +857,25 @@ double measure_fp64_peak_tflops() {
    cudaFree(d);
    const double flops = 2.0 * 8.0 * iters * (double)threads * blocks;
    return flops / (best * 1e-3) / 1e12;
+}
+
+// Loads every kernel of the engine on the current device and lets each take up to the device's
+// opt-in shared memory per block. The shared-memory limit is a process-wide attribute of a
+// kernel: set per launch (with the launch's own size), one caller thread could lower it between
+// another thread's setting and launch, which failed that launch ("invalid argument"). It is
+// therefore raised once, here, before any handle launches; launches pass only their own size.
+cudaError_t preload_kernels() {
+   cudaError_t e;
+   const int smax = max_dyn_smem();
+   const void *fns[] = {(const void *)k_prim<1>, (const void *)k_prim<4>, (const void *)k_prim<8>,
+                        (const void *)k_prim<32>, (const void *)k_prim2<true>, (const void *)k_prim2<false>,
+                        (const void *)k_group, (const void *)k_group_lane};
+   for (const void *f : fns)
+      if ((e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smax)) != cudaSuccess) return e;
+   cudaFuncAttributes a;
+   if ((e = cudaFuncGetAttributes(&a, (const void *)k_fp64_fma)) != cudaSuccess) return e;
+   if ((e = prim3_preload(smax)) != cudaSuccess) return e;
+   return group3_preload();
 }
 
 // ---------------------------------------------------------------------------------------

@@ -58,6 +58,8 @@ int prim_team_size(const ClassPlan &hp);
 constexpr size_t kNoAllocScratchDoubles = (size_t)8 * 1024 * 1024;   // 64 MiB
 constexpr int kMaxDevices = 64;
 cudaError_t noalloc_scratch(double **ptr);
+// loads every kernel on the current device (once per device, from libgint_init)
+cudaError_t preload_kernels();
 // sustained FP64 FMA rate of this GPU (TFLOP/s), from a dependent-FMA kernel
 double measure_fp64_peak_tflops();
 

@@ -267,9 +267,6 @@ cudaError_t launch_one(const DevCtx &ctx, const BatchArgs &bt, cudaStream_t st) 
    const int maxw = Sh::THREADS / 32;
    const int nw = (int)std::max<size_t>(1, std::min<size_t>(maxw, (budget - std::min(budget, neigh_bytes)) / warp_bytes));
    const size_t smem = neigh_bytes + warp_bytes * nw;
-   cudaError_t e = cudaFuncSetAttribute(k_prim3<LA, LB, LC, LD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)smem);
-   if (e != cudaSuccess) return e;
    const long nchunk = ((long)bt.nprm + Sh::CP - 1) / Sh::CP;
    const long blocks = std::max(1L, std::min((nchunk + nw - 1) / nw, 148L * 24));
    k_prim3<LA, LB, LC, LD><<<(unsigned)blocks, nw * 32, smem, st>>>(ctx, bt);
@@ -292,6 +289,22 @@ struct PartTable {
    }
 };
 
+// loads every kernel of this part and raises its shared-memory limit to smax
+template <int I>
+struct PartPreload {
+   static cudaError_t run(int smax) {
+      if constexpr (I >= kVrrGenCount) {
+         return cudaSuccess;
+      } else {
+         constexpr int c = kVrrGenClasses[I];
+         cudaError_t e = cudaFuncSetAttribute(k_prim3<(c >> 6) & 3, (c >> 4) & 3, (c >> 2) & 3, c & 3>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize, smax);
+         if (e != cudaSuccess) return e;
+         return PartPreload<I + kPrim3Parts>::run(smax);
+      }
+   }
+};
+
 }  // namespace
 
 #define PRIM3_CAT2(a, b) a##b
@@ -302,7 +315,19 @@ bool PRIM3_CAT(prim3_launch_part, PRIM3_PART)(const DevCtx &ctx, const BatchArgs
    return PartTable<PRIM3_PART>::launch(bt.cls, ctx, bt, st, err);
 }
 
+cudaError_t PRIM3_CAT(prim3_preload_part, PRIM3_PART)(int smax) { return PartPreload<PRIM3_PART>::run(smax); }
+
 #if PRIM3_PART == 0
+cudaError_t prim3_preload(int smax) {
+   cudaError_t (*parts[])(int) = {prim3_preload_part0, prim3_preload_part1, prim3_preload_part2, prim3_preload_part3,
+                               prim3_preload_part4, prim3_preload_part5, prim3_preload_part6, prim3_preload_part7};
+   for (auto f : parts) {
+      cudaError_t e = f(smax);
+      if (e != cudaSuccess) return e;
+   }
+   return cudaSuccess;
+}
+
 bool prim3_launch(const DevCtx &ctx, const BatchArgs &bt, cudaStream_t st, cudaError_t *err) {
    static_assert(kPrim3Parts == 8, "one call per part below");
    return prim3_launch_part0(ctx, bt, st, err) || prim3_launch_part1(ctx, bt, st, err) ||

@@ -74,6 +74,9 @@ def driver():
         lib.gd_build_K_subset.restype = ctypes.c_double
         lib.gd_build_K_subset.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _D, _D,
                                           ctypes.POINTER(ctypes.c_long), ctypes.c_long, _D]
+        lib.gd_build_K_mt.restype = ctypes.c_double
+        lib.gd_build_K_mt.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
+                                      _D, _D, ctypes.POINTER(ctypes.c_long), ctypes.c_long, _D]
         lib.gd_get_coeffs.restype = ctypes.c_int
         lib.gd_get_coeffs.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D, ctypes.POINTER(ctypes.c_int)]
         lib.gd_teardown.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
@@ -208,3 +211,34 @@ class Session:
             self.h = None
 
 
+
+
+class MultiSession:
+    """nthreads handles of one library, driven by nthreads host threads (one handle per thread,
+    as a caller with one handle per OpenMP thread uses the C-ABI); each thread streams a
+    contiguous share of the set quartets and the threads' K are summed."""
+
+    def __init__(self, api, wl, nthreads, max_mem_mb=1000):
+        self.api, self.wl, self.n = api, wl, int(nthreads)
+        self.hs = [driver().gd_setup(wl._w, api._a, max_mem_mb) for _ in range(self.n)]
+
+    def build_K(self, P=None, idx=None):
+        """One K build over all set quartets, or over the listed ones. Returns (K_flat, wall_ms,
+        thread 0's [setP, stream, getK] ms)."""
+        K = np.zeros(self.wl.info["flat_size"])
+        t = np.zeros(3)
+        Pp = None if P is None else _dp(np.ascontiguousarray(P, dtype=np.float64))
+        arr = (ctypes.c_void_p * self.n)(*self.hs)
+        if idx is None:
+            ip, n = None, 0
+        else:
+            idx = np.ascontiguousarray(idx, dtype=np.int64)
+            ip, n = idx.ctypes.data_as(ctypes.POINTER(ctypes.c_long)), idx.size
+        ms = driver().gd_build_K_mt(self.wl._w, self.api._a, arr, self.n, Pp, _dp(K), ip, n, _dp(t))
+        return K, ms, t
+
+    def close(self):
+        for h in self.hs:
+            if h:
+                driver().gd_teardown(self.api._a, h)
+        self.hs = []

@@ -134,3 +134,18 @@ def test_out_of_range_update_is_an_error(engine_so):
     code, msg = g.last_error()
     assert code == 3 and "outside" in msg
     g.close()
+
+
+@pytest.mark.gpu
+def test_multithreaded_caller_matches_oracle(engine_so, oracle_path):
+    """Four host threads with one engine handle each on one GPU (contiguous shares of the set
+    quartets, K summed): the oracle's K within the FP64 tolerance."""
+    from libgint_b200.workload import MultiSession
+    wl = Workload("periodic_l2_small")
+    m = MultiSession(Api(engine_so), wl, 4)
+    Ke, ms, _ = m.build_K()
+    m.close()
+    Ko, _, _ = _k(oracle_path, wl)
+    rel = np.abs(Ke - Ko).max() / np.abs(Ko).max()
+    print(f"4 caller threads: engine vs oracle {rel:.3e}, {ms:.1f} ms")
+    assert rel <= TOL, rel

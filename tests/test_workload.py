@@ -3,7 +3,7 @@ import numpy as np
 import pytest
 
 from conftest import ORACLE_SO
-from libgint_b200.workload import Api, Session, Workload
+from libgint_b200.workload import Api, MultiSession, Session, Workload
 
 
 def test_deterministic():
@@ -79,3 +79,28 @@ def test_exchange_energy_negative_and_stable():
     Ka = s.build_K_subset(np.arange(0, nq, 2))[0]
     Kb = s.build_K_subset(np.arange(1, nq, 2))[0]
     assert np.abs(Ka + Kb - K).max() <= 1e-12 * np.abs(K).max()
+
+
+def test_multithreaded_caller_sums_to_single_handle():
+    """Three host threads with one handle each (contiguous shares of the set quartets) give the
+    single-handle K up to summation order."""
+    import ctypes
+    ora = Api(ORACLE_SO)
+    w = Workload("small_l2")
+    s1 = Session(ora, w)
+    K1 = s1.build_K()[0]
+    s1.close()
+    m = MultiSession(ora, w, 3)
+    set_threads = ora.symbol("oracle_set_threads", None, [ctypes.c_void_p, ctypes.c_int])
+    for h in m.hs:
+        set_threads(h, 1)
+    Km, ms, _ = m.build_K()
+    idx = np.arange(0, w.info["n_setq"], 2)
+    Ks, _, _ = m.build_K(idx=idx)
+    m.close()
+    assert ms > 0
+    assert np.abs(Km - K1).max() <= 1e-13 * np.abs(K1).max()
+    s2 = Session(ora, w)
+    K2 = s2.build_K_subset(idx)[0]
+    s2.close()
+    assert np.abs(Ks - K2).max() <= 1e-13 * np.abs(K2).max()
