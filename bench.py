@@ -47,8 +47,10 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--host-threads", type=int, default=min(8, os.cpu_count() or 1),
+    ap.add_argument("--host-threads", type=int, default=min(16, os.cpu_count() or 1),
                     help="caller threads (one handle each) of the end-to-end leg")
+    ap.add_argument("--host-mem-mb", type=int, default=300,
+                    help="libgint_set_max_mem of each end-to-end handle (smaller batches start the GPU sooner)")
     return ap.parse_args()
 
 
@@ -277,11 +279,24 @@ def run_ours(args, world, rank, local):
             if line.startswith("bytes_per_launch:"):
                 traffic = float(line.split(":")[1])
 
-    # 4) e2e through the C-ABI with host buffers: set_P, add_* stream, get_K, driven as a caller
+    # 4) CPU baseline (rank 0 at N=1): the oracle on a strided sample, plus parity on it
+    cpu = None
+    parity = None
+    if rank == 0 and world == 1:
+        cb = cpu_oracle_sample(wl, args.cpu_seconds)
+        Ke, _, _ = sess.build_K_subset(cb["idx"])
+        parity = float(np.abs(Ke - cb["K"]).max() / max(1e-300, np.abs(cb["K"]).max()))
+        cpu = {"value": cb["value"], "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+               "sample": cb["sample"]}
+    # the recording session's device batches and pinned queues are released before the
+    # end-to-end leg, which sets up its own handles
+    sess.close()
+
+    # 5) e2e through the C-ABI with host buffers: set_P, add_* stream, get_K, driven as a caller
     #    with one handle per host thread does (each thread streams a contiguous share of this
     #    rank's set quartets; the threads' K are summed on the host)
     from libgint_b200.workload import MultiSession
-    msess = MultiSession(api, wl, args.host_threads)
+    msess = MultiSession(api, wl, args.host_threads, max_mem_mb=args.host_mem_mb)
 
     def h2d_total():
         tot = 0
@@ -294,12 +309,13 @@ def run_ours(args, world, rank, local):
         msess.build_K(idx=idx)
     barrier()
     h2d0 = h2d_total()
-    e2e_ms = []
+    e2e_ms, e2e_parts = [], []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        K, _, _ = msess.build_K(idx=idx)
+        K, _, tparts = msess.build_K(idx=idx)
         K = sum_K(K)
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        e2e_parts.append(tparts)
     barrier()
     for hh in msess.hs:
         e = lib.libgint_last_error(ctypes.c_void_p(hh))
@@ -313,16 +329,6 @@ def run_ours(args, world, rank, local):
     d2h = wl.info["flat_size"] * 8 * args.host_threads
     ex = wl.exchange_energy(K)
 
-    # 5) CPU baseline (rank 0 at N=1): the oracle on a strided sample, plus parity on it
-    cpu = None
-    parity = None
-    if rank == 0 and world == 1:
-        cb = cpu_oracle_sample(wl, args.cpu_seconds)
-        Ke, _, _ = sess.build_K_subset(cb["idx"])
-        parity = float(np.abs(Ke - cb["K"]).max() / max(1e-300, np.abs(cb["K"]).max()))
-        cpu = {"value": cb["value"], "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-               "sample": cb["sample"]}
-    sess.close()
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -338,7 +344,9 @@ def run_ours(args, world, rank, local):
             "E_x": ex,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms_step,
-                    "host_threads": args.host_threads},
+                    "host_threads": args.host_threads,
+                    "slowest_thread_ms": float(np.mean([t[3] for t in e2e_parts])),
+                    "k_sum_ms": float(np.mean([t[4] for t in e2e_parts]))},
             "gpu_launches": int(launches),
             "roofline": {"bound": "fp64", "kernel": "k_prim (Fm + VRR + image sum)",
                          "achieved": prim_tflops, "peak": peak, "unit": "TFLOP/s",

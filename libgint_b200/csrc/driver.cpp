@@ -787,14 +787,10 @@ static double build_K_impl(const gd_workload *w, gd_api *a, void *h, const doubl
    return ms(t0, t3);
 }
 
-// One K build by nh host threads, thread t driving handles[t] (each set up by gd_setup) over a
-// contiguous share of the set quartets (all of them, or idx[0..n_idx) when idx is given) with
-// about the same number of primitive quartets, as a
-// caller with one handle per OpenMP thread does; the threads' K are summed into K. Returns wall
-// ms; times[0..2] are thread 0's set_P / stream / get_K (ms).
-double gd_build_K_mt(const gd_workload *w, gd_api *a, void **handles, int nh, const double *P, double *K,
-                     const long *idx, long n_idx, double *times) {
-   using clk = std::chrono::steady_clock;
+// Split of a K build over nh caller threads: cut[0..nh] bounds contiguous shares of the set
+// quartets (all of them, or idx[0..n_idx) when idx is given) with about the same number of
+// primitive quartets each.
+void gd_mt_split(const gd_workload *w, const long *idx, long n_idx, int nh, long *cut) {
    const long nq = idx ? n_idx : (long)w->setq.size();
    std::vector<double> cum(nq + 1, 0.0);
    for (long q = 0; q < nq; q++) {
@@ -803,23 +799,42 @@ double gd_build_K_mt(const gd_workload *w, gd_api *a, void **handles, int nh, co
       for (uint32_t hh = s.shell_begin; hh < s.shell_end; hh++) np += w->shells[hh].prm_end - w->shells[hh].prm_begin;
       cum[q + 1] = cum[q] + (double)np;
    }
-   std::vector<long> cut(nh + 1, nq);
    cut[0] = 0;
+   cut[nh] = nq;
    for (int t = 1; t < nh; t++)
       cut[t] = (long)(std::lower_bound(cum.begin(), cum.end(), cum[nq] * t / nh) - cum.begin());
-   std::vector<std::vector<double>> Ks(nh, std::vector<double>(w->flat_size, 0.0));
-   std::vector<double> tt(3 * nh, 0.0);
+}
+
+// One K build by nh host threads, thread t driving handles[t] (each set up by gd_setup) over the
+// set quartets [cut[t], cut[t+1]) (positions in idx[] when idx is given; see gd_mt_split), as a
+// caller with one handle per OpenMP thread does; the threads' K are summed into K. Returns wall
+// ms; times[0..2] are thread 0's set_P / stream / get_K, times[3] the slowest thread's build and
+// times[4] the summation (ms).
+double gd_build_K_mt(const gd_workload *w, gd_api *a, void **handles, int nh, const double *P, double *K,
+                     const long *idx, const long *cut, double *times) {
+   using clk = std::chrono::steady_clock;
+   auto ms = [](clk::time_point x, clk::time_point y) { return std::chrono::duration<double, std::milli>(y - x).count(); };
+   std::vector<std::vector<double>> Ks(nh);
+   std::vector<double> tt(3 * nh, 0.0), tw(nh, 0.0);
    auto t0 = clk::now();
    std::vector<std::thread> th;
    for (int t = 0; t < nh; t++)
-      th.emplace_back([&, t]() { build_K_impl(w, a, handles[t], P, Ks[t].data(), cut[t], cut[t + 1], idx, &tt[3 * t]); });
+      th.emplace_back([&, t]() {
+         Ks[t].assign(w->flat_size, 0.0);
+         tw[t] = build_K_impl(w, a, handles[t], P, Ks[t].data(), cut[t], cut[t + 1], idx, &tt[3 * t]);
+      });
    for (auto &x : th) x.join();
+   auto t1 = clk::now();
    std::fill(K, K + w->flat_size, 0.0);
    for (int t = 0; t < nh; t++)
       for (size_t i = 0; i < w->flat_size; i++) K[i] += Ks[t][i];
-   auto t1 = clk::now();
-   if (times) for (int i = 0; i < 3; i++) times[i] = tt[i];
-   return std::chrono::duration<double, std::milli>(t1 - t0).count();
+   auto t2 = clk::now();
+   if (times) {
+      for (int i = 0; i < 3; i++) times[i] = tt[i];
+      times[3] = *std::max_element(tw.begin(), tw.end());
+      times[4] = ms(t1, t2);
+   }
+   return ms(t0, t2);
 }
 
 void gd_teardown(gd_api *a, void *h) { if (a->destroy) a->destroy(h); }

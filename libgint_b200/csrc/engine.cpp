@@ -249,7 +249,8 @@ struct Handle {
    std::vector<SetFast> fast;
    bool basis_dirty = true, ent_dirty = true;
    // device-resident data
-   DBuf d_pool, d_ents, d_neighs, d_C0, d_lut, d_bw, d_ft, d_plans, d_err;
+   DBuf d_pool, d_ents, d_neighs, d_C0, d_lut, d_bw, d_ft, d_plans, d_err, d_vops;
+   std::vector<VOp> vops;           // precompiled VRR instructions of all classes
    DBuf d_P[2], d_K[2];
    int nspin = 0;
    size_t FP_size = 0;
@@ -344,6 +345,8 @@ static bool upload_tables(Handle *h) {
    if (!h->plans_ready) {
       if (!ensure(h, h->d_plans, sizeof(ClassPlan) * 256, "plans")) return false;
       if (!h2d(h, h->d_plans.p, h->plans, sizeof(ClassPlan) * 256, "plans")) return false;
+      if (!ensure(h, h->d_vops, h->vops.size() * sizeof(VOp), "VRR instructions")) return false;
+      if (!h2d(h, h->d_vops.p, h->vops.data(), h->vops.size() * sizeof(VOp), "VRR instructions")) return false;
       std::vector<uint8_t> lut;
       std::vector<double> bw;
       make_patch_tables(lut, bw);
@@ -467,6 +470,7 @@ static DevCtx make_ctx(Handle *h) {
    c.FP_size = h->FP_size;
    c.err = (int *)h->d_err.p;
    c.cnt = h->counting ? (unsigned long long *)h->d_cnt.p : nullptr;
+   c.vops = (const VOp *)h->d_vops.p;
    return c;
 }
 
@@ -730,7 +734,10 @@ void *libgint_create_handle(void) {
    Handle *h = new Handle();
    h->prm_tmp.reserve(65536);
    for (int c = 0; c < 256; c++) h->open_of[c] = -1;
-   for (int c = 0; c < 256; c++) build_class_plan(c >> 6, (c >> 4) & 3, (c >> 2) & 3, c & 3, h->plans[c]);
+   for (int c = 0; c < 256; c++) {
+      build_class_plan(c >> 6, (c >> 4) & 3, (c >> 2) & 3, c & 3, h->plans[c]);
+      build_vops(h->plans[c], h->vops);
+   }
    return h;
 }
 
@@ -1224,7 +1231,7 @@ void libgint_destroy_handle(void *hh) {
    }
    for (auto &rb : h->recs) release(rb.rec);
    release(h->rec_ac); release(h->rec_gscr); release(h->d_cnt);
-   DBuf *bufs[] = {&h->d_pool, &h->d_ents, &h->d_neighs, &h->d_C0, &h->d_lut, &h->d_bw, &h->d_ft,
+   DBuf *bufs[] = {&h->d_pool, &h->d_ents, &h->d_neighs, &h->d_C0, &h->d_lut, &h->d_bw, &h->d_ft, &h->d_vops,
                    &h->d_plans, &h->d_err, &h->d_P[0], &h->d_P[1], &h->d_K[0], &h->d_K[1]};
    for (DBuf *b : bufs) release(*b);
    for (int w = 0; w < kWorkStreams; w++) {

@@ -65,6 +65,18 @@ struct HOp {
    int nelem;
 };
 
+// One VRR element as a precompiled instruction (see build_vops in plan.cpp): the element's
+// workspace offset, its inputs, the pqz slot of its first factor and its integer multipliers.
+//   A form (kind 0):  w[out] = z[zA] w[i0] + z[zA+3] w[i1] + f1 (z[12] w[i2] + z[13] w[i3])
+//   C form (kind 1):  w[out] = z[zA] w[i0] + z[zA+3] w[i1] + f1 (z[14] w[i2] + z[15] w[i3])
+//                              + f2 z[16] w[i4]
+// Absent inputs point at a zero slot (offset V) and carry a zero multiplier.
+struct VOp {
+   int16_t out, i0, i1, i2, i3, i4;
+   uint8_t zA, kind;
+   int8_t f1, f2;
+};
+
 constexpr int kMaxVB = 64;
 constexpr int kMaxLev = 16;
 constexpr int kMaxTgt = 16;
@@ -83,6 +95,8 @@ struct ClassPlan {
    int tg_voff[kMaxTgt * 4], tg_soff[kMaxTgt * 4], tg_n[kMaxTgt * 4], tg_e[kMaxTgt * 4], tg_f[kMaxTgt * 4];
    int nhop, nhlev;
    int hlev_off[kMaxLev + 1];
+   int vop_off, nvop;      // the class's VRR instructions in the engine's VOp table
+   int vop_lev[kMaxLev + 1];   // level l (1..nlev) is instructions [vop_lev[l-1], vop_lev[l])
    int want00;             // la == 0 && lc == 0: the (00|00) target collects every image
    int s00;                // offset of the (00|00) target in S (if want00)
    VBlock vb[kMaxVB];

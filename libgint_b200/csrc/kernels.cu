@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cstdint>
+#include <cstring>
 #include <mutex>
 #include "engine_types.h"
 #include "kernels.h"
@@ -97,6 +98,21 @@ static __device__ __forceinline__ void vrr_elem(const VBlock &b, int e, double *
    vrr_elem_s<1>(b, e, ws, pqz);
 }
 
+// One level of the precompiled VRR (VOp, see build_vops): instructions [e0, e1) spread over the
+// lanes of a team; ws holds a zero at offset V.
+static __device__ __forceinline__ void vops_level(const VOp *__restrict__ vop, int e0, int e1, int lane, int stride,
+                                                  double *ws, const double *pqz) {
+   for (int e = e0 + lane; e < e1; e += stride) {
+      const int4 r = __ldg(reinterpret_cast<const int4 *>(vop + e));
+      VOp o;
+      memcpy(&o, &r, sizeof(VOp));
+      double v = pqz[o.zA] * ws[o.i0] + pqz[o.zA + 3] * ws[o.i1];
+      if (o.f1) v += o.f1 * (pqz[12 + 2 * o.kind] * ws[o.i2] + pqz[13 + 2 * o.kind] * ws[o.i3]);
+      if (o.f2) v += o.f2 * pqz[16] * ws[o.i4];
+      ws[o.out] = v;
+   }
+}
+
 template <int TS>
 static __device__ __forceinline__ void team_sync(unsigned mask) {
    if (TS > 1) __syncwarp(mask);
@@ -120,13 +136,14 @@ __global__ void __launch_bounds__(256) k_prim(DevCtx ctx, BatchArgs bt, int team
    const int team = threadIdx.x / TS, lane = threadIdx.x % TS, nteam = blockDim.x / TS;
    double *tws = smem + plan_doubles + (size_t)team * team_doubles;
    const int L = pl->L, V = pl->V, S = pl->S;
-   double *ws = tws;                  // VRR workspace [V]
-   double *acc = tws + V;             // image-summed targets [S]
+   double *ws = tws;                  // VRR workspace [V] and a zero slot
+   double *acc = tws + V + 1;         // image-summed targets [S]
    double *pqz = acc + S;             // 17 factors of the image being processed
    double *fmx = pqz + 17;            // per-lane Fm [TS][L+1]
    const unsigned wl = (threadIdx.x & 31) / TS * TS;
    const unsigned mask = (TS >= 32) ? 0xffffffffu : (((1u << TS) - 1u) << wl);
 
+   if (lane == 0) ws[V] = 0.0;
    for (uint32_t p = blockIdx.x * nteam + team; p < bt.nprm; p += gridDim.x * nteam) {
       PrimGeo g;
       prim_geometry(ctx, bt.shells[bt.prm_shell[p]], bt.prm[p], g);
@@ -172,14 +189,7 @@ __global__ void __launch_bounds__(256) k_prim(DevCtx ctx, BatchArgs bt, int team
             }
             team_sync<TS>(mask);
             for (int lv = 1; lv <= pl->nlev; lv++) {
-               const int b0 = pl->lev_off[lv - 1], b1 = pl->lev_off[lv];
-               int tot = 0;
-               for (int bb = b0; bb < b1; bb++) tot += pl->vb[bb].nelem;
-               for (int e = lane; e < tot; e += TS) {
-                  int bb = b0, ee = e;
-                  while (ee >= pl->vb[bb].nelem) { ee -= pl->vb[bb].nelem; bb++; }
-                  vrr_elem(pl->vb[bb], ee, ws, pqz);
-               }
+               vops_level(ctx.vops + pl->vop_off, pl->vop_lev[lv - 1], pl->vop_lev[lv], lane, TS, ws, pqz);
                team_sync<TS>(mask);
             }
             for (int t = 0; t < pl->ntg; t++) {
@@ -255,10 +265,11 @@ __global__ void __launch_bounds__(256) k_prim2(DevCtx ctx, BatchArgs bt, int cp,
    int *q2i = reinterpret_cast<int *>(q1t + 64);                      // [64] pair index
    double *q2f = q1t + 64 + 32;                                       // [64][LF] Fm
    double *pqz = q2f + 64 * LF;                                       // [17][32] (lane) or [17]
-   double *ws = pqz + (LANE_VRR ? 17 * 32 : 18);                      // [V][32] (lane) or [V]
+   double *ws = pqz + (LANE_VRR ? 17 * 32 : 18);                      // [V][32] (lane) or [V] + zero
    const bool need_vrr = !(pl->want00 && pl->ntg == 1);
    const unsigned below = (1u << lane) - 1u;
    unsigned long long c_cheb = 0, c_boys = 0, c_vrr = 0;
+   if (!LANE_VRR && lane == 0) ws[pl->V] = 0.0;
 
    const uint32_t nchunk = (bt.nprm + cp - 1) / cp;
    for (uint32_t ch = blockIdx.x * nwarp + warp; ch < nchunk; ch += gridDim.x * nwarp) {
@@ -331,14 +342,7 @@ __global__ void __launch_bounds__(256) k_prim2(DevCtx ctx, BatchArgs bt, int cp,
                for (int q = lane; q < n00; q += 32) ws[q] = q2f[s * LF + q];
                __syncwarp();
                for (int lv = 1; lv <= pl->nlev; lv++) {
-                  const int b0 = pl->lev_off[lv - 1], b1 = pl->lev_off[lv];
-                  int tot = 0;
-                  for (int bb = b0; bb < b1; bb++) tot += pl->vb[bb].nelem;
-                  for (int e = lane; e < tot; e += 32) {
-                     int bb = b0, ee = e;
-                     while (ee >= pl->vb[bb].nelem) { ee -= pl->vb[bb].nelem; bb++; }
-                     vrr_elem(pl->vb[bb], ee, ws, pqz);
-                  }
+                  vops_level(ctx.vops + pl->vop_off, pl->vop_lev[lv - 1], pl->vop_lev[lv], lane, 32, ws, pqz);
                   __syncwarp();
                }
                double *ap = acc + (size_t)p * S;
@@ -681,7 +685,7 @@ static int max_dyn_smem() {
 template <int TS>
 static cudaError_t launch_prim_t(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan &hp, cudaStream_t st) {
    const int L = hp.L;
-   int team_doubles = hp.V + hp.S + 17 + TS * (L + 1);
+   int team_doubles = hp.V + 1 + hp.S + 17 + TS * (L + 1);
    team_doubles = (team_doubles + 1) & ~1;
    const int budget = std::min(max_dyn_smem(), 200 * 1024);
    const size_t plan_bytes = (size_t)plan_smem_doubles() * 8;
@@ -708,7 +712,7 @@ static void prim2_shape(const ClassPlan &hp, bool lane_vrr, int *cp, size_t *war
    int c = std::max(1, std::min(32, 2048 / std::max(1, hp.S)));
    const size_t geo = (sizeof(PrimGeo) / 8);
    size_t w = geo * c + c + (size_t)c * hp.S + 32 + 64 + 32 + 64 * (size_t)(hp.L + 1) +
-              (lane_vrr ? 17 * 32 + 32 * (size_t)hp.V : 18 + (size_t)hp.V);
+              (lane_vrr ? 17 * 32 + 32 * (size_t)hp.V : 18 + (size_t)hp.V + 2);
    *cp = c;
    *warp_doubles = (w + 1) & ~(size_t)1;
 }

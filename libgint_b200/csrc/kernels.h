@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 #include "engine_types.h"
 
 namespace gint {
@@ -31,6 +32,7 @@ struct DevCtx {
    size_t FP_size;
    int *err;
    unsigned long long *cnt;   // optional event counters per class [256][4], or null
+   const VOp *vops;           // precompiled VRR instructions of every class (build_vops)
 };
 
 // One class-sorted segment of a batch (device pointers).
@@ -48,6 +50,7 @@ struct BatchArgs {
 };
 
 bool build_class_plan(int la, int lb, int lc, int ld, ClassPlan &p);
+void build_vops(ClassPlan &p, std::vector<VOp> &out);
 cudaError_t upload_constant_tables(const double *c2s_l0to3, const double *symm5);
 cudaError_t launch_prim(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan &hp, cudaStream_t st);
 cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan &hp, cudaStream_t st);

@@ -10,6 +10,7 @@
 //  * HRR: ket steps (e0|c d) for d = 1..ld, then bra steps (a b|lc ld) for b = 1..lb.
 #include <algorithm>
 #include <cstring>
+#include <vector>
 #include "engine_types.h"
 
 namespace gint {
@@ -134,6 +135,73 @@ bool build_class_plan(int la, int lb, int lc, int ld, ClassPlan &p) {
    p.out_off = bloc[la][lb];
    p.H = hoff;
    return true;
+}
+
+// ---- precompiled VRR instructions -------------------------------------------------------
+static void cart_exps(int l, int i, int e[3]) {
+   int a = 0;
+   while ((a + 1) * (a + 2) / 2 <= i) a++;
+   e[0] = l - a; e[2] = i - a * (a + 1) / 2; e[1] = a - e[2];
+}
+static int cart_idx(const int e[3]) { const int a = e[1] + e[2]; return a * (a + 1) / 2 + e[2]; }
+static int first_dir(const int e[3]) { return e[0] ? 0 : (e[1] ? 1 : 2); }
+static int lowered_idx(const int e[3], int d, int n) { int f[3] = {e[0], e[1], e[2]}; f[d] -= n; return cart_idx(f); }
+
+// Appends the VRR of class p as one instruction per workspace element, level by level, with the
+// same inputs and multipliers as the element formulas of the interpreted kernels
+// (reference VRR1..VRR6, src/compute_VRR.cpp:111-345), and records the level boundaries.
+void build_vops(ClassPlan &p, std::vector<VOp> &out) {
+   const int16_t zero = (int16_t)p.V;   // the workspace's zero slot
+   p.vop_off = (int)out.size();
+   p.vop_lev[0] = 0;
+   for (int lv = 1; lv <= p.nlev; lv++) {
+      for (int bb = p.lev_off[lv - 1]; bb < p.lev_off[lv]; bb++) {
+         const VBlock &b = p.vb[bb];
+         const int a = b.a, c = b.c, na = ncart(a), nc = ncart(c);
+         for (int mm = 0; mm < b.nm; mm++) for (int i = 0; i < na; i++) for (int k = 0; k < nc; k++) {
+            const int m = b.lo + mm;
+            VOp o;
+            o.out = (int16_t)(b.off + (mm * na + i) * nc + k);
+            o.i2 = o.i3 = o.i4 = zero;
+            o.f1 = o.f2 = 0;
+            int ea[3];
+            cart_exps(a, i, ea);
+            if (c == 0) {
+               const int d = first_dir(ea), im = lowered_idx(ea, d, 1), na1 = ncart(a - 1);
+               o.kind = 0; o.zA = (uint8_t)d;
+               o.i0 = (int16_t)(b.in1 + (m - b.lo1) * na1 + im);
+               o.i1 = (int16_t)(b.in1 + (m + 1 - b.lo1) * na1 + im);
+               if (ea[d] >= 2) {
+                  const int iw = lowered_idx(ea, d, 2), na2 = ncart(a - 2);
+                  o.f1 = (int8_t)(ea[d] - 1);
+                  o.i2 = (int16_t)(b.in2 + (m - b.lo2) * na2 + iw);
+                  o.i3 = (int16_t)(b.in2 + (m + 1 - b.lo2) * na2 + iw);
+               }
+            } else {
+               int ec[3];
+               cart_exps(c, k, ec);
+               const int d = first_dir(ec), km = lowered_idx(ec, d, 1), nc1 = ncart(c - 1);
+               o.kind = 1; o.zA = (uint8_t)(6 + d);
+               o.i0 = (int16_t)(b.in1 + ((m - b.lo1) * na + i) * nc1 + km);
+               o.i1 = (int16_t)(b.in1 + ((m + 1 - b.lo1) * na + i) * nc1 + km);
+               if (ec[d] >= 2) {
+                  const int kw = lowered_idx(ec, d, 2), nc2 = ncart(c - 2);
+                  o.f1 = (int8_t)(ec[d] - 1);
+                  o.i2 = (int16_t)(b.in2 + ((m - b.lo2) * na + i) * nc2 + kw);
+                  o.i3 = (int16_t)(b.in2 + ((m + 1 - b.lo2) * na + i) * nc2 + kw);
+               }
+               if (a > 0 && ea[d] >= 1) {
+                  const int im = lowered_idx(ea, d, 1);
+                  o.f2 = (int8_t)ea[d];
+                  o.i4 = (int16_t)(b.in3 + ((m + 1 - b.lo3) * ncart(a - 1) + im) * nc1 + km);
+               }
+            }
+            out.push_back(o);
+         }
+      }
+      p.vop_lev[lv] = (int)out.size() - p.vop_off;
+   }
+   p.nvop = (int)out.size() - p.vop_off;
 }
 
 }  // namespace gint

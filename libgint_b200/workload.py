@@ -76,7 +76,10 @@ def driver():
                                           ctypes.POINTER(ctypes.c_long), ctypes.c_long, _D]
         lib.gd_build_K_mt.restype = ctypes.c_double
         lib.gd_build_K_mt.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
-                                      _D, _D, ctypes.POINTER(ctypes.c_long), ctypes.c_long, _D]
+                                      _D, _D, ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_long), _D]
+        lib.gd_mt_split.restype = None
+        lib.gd_mt_split.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_long), ctypes.c_long, ctypes.c_int,
+                                    ctypes.POINTER(ctypes.c_long)]
         lib.gd_get_coeffs.restype = ctypes.c_int
         lib.gd_get_coeffs.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D, ctypes.POINTER(ctypes.c_int)]
         lib.gd_teardown.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
@@ -224,17 +227,26 @@ class MultiSession:
 
     def build_K(self, P=None, idx=None):
         """One K build over all set quartets, or over the listed ones. Returns (K_flat, wall_ms,
-        thread 0's [setP, stream, getK] ms)."""
+        times): times[0..2] thread 0's set_P / stream / get_K, [3] the slowest thread's build,
+        [4] the summation of the threads' K (ms). The split over threads is computed once per
+        set-quartet list."""
         K = np.zeros(self.wl.info["flat_size"])
-        t = np.zeros(3)
+        t = np.zeros(5)
         Pp = None if P is None else _dp(np.ascontiguousarray(P, dtype=np.float64))
         arr = (ctypes.c_void_p * self.n)(*self.hs)
         if idx is None:
-            ip, n = None, 0
+            ip, n, key = None, 0, None
         else:
             idx = np.ascontiguousarray(idx, dtype=np.int64)
-            ip, n = idx.ctypes.data_as(ctypes.POINTER(ctypes.c_long)), idx.size
-        ms = driver().gd_build_K_mt(self.wl._w, self.api._a, arr, self.n, Pp, _dp(K), ip, n, _dp(t))
+            ip, n, key = idx.ctypes.data_as(ctypes.POINTER(ctypes.c_long)), idx.size, (idx.size, int(idx[0]) if idx.size else 0,
+                                                                                          int(idx[-1]) if idx.size else 0)
+        if getattr(self, "_cut_key", "unset") != key:
+            self._cut = np.zeros(self.n + 1, dtype=np.int64)
+            driver().gd_mt_split(self.wl._w, ip, n, self.n, self._cut.ctypes.data_as(ctypes.POINTER(ctypes.c_long)))
+            self._cut_key = key
+            self._idx = idx
+        ms = driver().gd_build_K_mt(self.wl._w, self.api._a, arr, self.n, Pp, _dp(K), ip,
+                                    self._cut.ctypes.data_as(ctypes.POINTER(ctypes.c_long)), _dp(t))
         return K, ms, t
 
     def close(self):
