@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--host-threads", type=int, default=min(16, os.cpu_count() or 1),
                     help="caller threads (one handle each) of the end-to-end leg")
+    ap.add_argument("--device-only", action="store_true",
+                    help="record and replay only (no end-to-end or CPU legs); prints the device line "
+                         "(for profiling a fixed number of identical K builds)")
     ap.add_argument("--host-mem-mb", type=int, default=300,
                     help="libgint_set_max_mem of each end-to-end handle (smaller batches start the GPU sooner)")
     return ap.parse_args()
@@ -279,6 +282,18 @@ def run_ours(args, world, rank, local):
             if line.startswith("bytes_per_launch:"):
                 traffic = float(line.split(":")[1])
 
+    if args.device_only:
+        # the record build, the warm-up and timed replays and the profiled replay: warmup + steps + 2
+        # identical K builds
+        sess.close()
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "ms_per_step": ms_per_step,
+                              "device_only": True, "k_builds": args.warmup + args.steps + 2,
+                              "kernel_ms_per_step": kt[0], "group_kernel_ms_per_step": kt[1]}), flush=True)
+        if pg:
+            torch.distributed.destroy_process_group()
+        return
+
     # 4) CPU baseline (rank 0 at N=1): the oracle on a strided sample, plus parity on it
     cpu = None
     parity = None
@@ -351,6 +366,8 @@ def run_ours(args, world, rank, local):
             "roofline": {"bound": "fp64", "kernel": "k_prim (Fm + VRR + image sum)",
                          "achieved": prim_tflops, "peak": peak, "unit": "TFLOP/s",
                          "frac": prim_tflops / peak if peak > 0 else None, "traffic": traffic,
+                         "traffic_unit": "DRAM bytes of the primitive kernels per K build (ncu, scaled; "
+                                         "profiles/launches_periodic_l2_small.md)",
                          "peak_source": "FP64 FMA rate measured by libgint_fp64_peak_tflops on this GPU",
                          "kernel_ms_per_step": kt[0], "group_kernel_ms_per_step": kt[1],
                          "flops_per_step": flops_prim, "images_evaluated": int(n_img)},

@@ -32,8 +32,16 @@ __device__ __forceinline__ double symm_factor(int i) {
    return i == 0 ? 2.0 : (i == 1 ? 1.0 : (i == 2 ? 0.5 : (i == 3 ? 0.25 : 0.0)));
 }
 
+// resident 128-thread blocks per SM the register budget is sized for: the kernel waits on
+// chains of dependent loads, so small classes trade registers for more warps in flight
 template <int LA, int LB, int LC, int LD>
-__global__ void __launch_bounds__(128) k_group3(DevCtx ctx, BatchArgs bt) {
+struct Group3Shape {
+   static constexpr int L = LA + LB + LC + LD;
+   static constexpr int MINB = L <= 1 ? 8 : (L == 2 ? 6 : 4);
+};
+
+template <int LA, int LB, int LC, int LD>
+__global__ void __launch_bounds__(128, Group3Shape<LA, LB, LC, LD>::MINB) k_group3(DevCtx ctx, BatchArgs bt) {
    using G = GrpGen<LA, LB, LC, LD>;
    constexpr int S = G::S, Nc = G::Nc, Ns = G::Ns;
    constexpr int nsb = 2 * LB + 1, nsc = 2 * LC + 1, nsd = 2 * LD + 1;
