@@ -249,7 +249,7 @@ struct Handle {
    std::vector<SetFast> fast;
    bool basis_dirty = true, ent_dirty = true;
    // device-resident data
-   DBuf d_pool, d_ents, d_neighs, d_C0, d_lut, d_bw, d_ft, d_plans, d_err, d_vops;
+   DBuf d_pool, d_ents, d_neighs, d_C0, d_lut, d_bw, d_ft, d_plans, d_err, d_vops, d_gtab;
    std::vector<VOp> vops;           // precompiled VRR instructions of all classes
    DBuf d_P[2], d_K[2];
    int nspin = 0;
@@ -358,11 +358,15 @@ static bool upload_tables(Handle *h) {
       if (!h2d(h, h->d_lut.p, lut.data(), lut.size(), "lut")) return false;
       if (!h2d(h, h->d_bw.p, bw.data(), bw.size() * 8, "bw")) return false;
       if (!h2d(h, h->d_ft.p, ft.data(), ft.size() * 8, "ftable")) return false;
-      if (!ck(h, cudaMemset(h->d_err.p, 0, sizeof(int) * 4), "err")) return false;
+      if (!ck(h, cudaMemsetAsync(h->d_err.p, 0, sizeof(int) * 4, h->stream), "err")) return false;
       double c2s[4][70];
       make_c2s(c2s);
       const double symm[5] = {2.0, 1.0, 0.5, 0.25, 0.0};
       if (!ck(h, upload_constant_tables(&c2s[0][0], symm), "constant tables")) return false;
+      std::vector<uint8_t> gtab(kGroupTabBytes);
+      build_group_tables(&c2s[0][0], gtab.data());
+      if (!ensure(h, h->d_gtab, kGroupTabBytes, "group tables")) return false;
+      if (!h2d(h, h->d_gtab.p, gtab.data(), kGroupTabBytes, "group tables")) return false;
       h->plans_ready = true;
       uploaded = true;
    }
@@ -471,6 +475,7 @@ static DevCtx make_ctx(Handle *h) {
    c.err = (int *)h->d_err.p;
    c.cnt = h->counting ? (unsigned long long *)h->d_cnt.p : nullptr;
    c.vops = (const VOp *)h->d_vops.p;
+   c.gtab = (const uint8_t *)h->d_gtab.p;
    return c;
 }
 
@@ -1231,7 +1236,7 @@ void libgint_destroy_handle(void *hh) {
    }
    for (auto &rb : h->recs) release(rb.rec);
    release(h->rec_ac); release(h->rec_gscr); release(h->d_cnt);
-   DBuf *bufs[] = {&h->d_pool, &h->d_ents, &h->d_neighs, &h->d_C0, &h->d_lut, &h->d_bw, &h->d_ft, &h->d_vops,
+   DBuf *bufs[] = {&h->d_pool, &h->d_ents, &h->d_neighs, &h->d_C0, &h->d_lut, &h->d_bw, &h->d_ft, &h->d_vops, &h->d_gtab,
                    &h->d_plans, &h->d_err, &h->d_P[0], &h->d_P[1], &h->d_K[0], &h->d_K[1]};
    for (DBuf *b : bufs) release(*b);
    for (int w = 0; w < kWorkStreams; w++) {

@@ -66,6 +66,8 @@ __global__ void __launch_bounds__(128, Group3Shape<LA, LB, LC, LD>::MINB) k_grou
             double T[S];
 #pragma unroll
             for (int j = 0; j < S; j++) T[j] = 0.0;
+            // two primitives per iteration so that the next one's loads overlap this one's FMAs
+#pragma unroll 2
             for (uint32_t ip = 0; ip < sh.nprm; ip++) {
                const uint32_t code = __ldg(bt.prm + sh.prm_off + ip);
                const double kp = __ldg(Ka + (code >> 24)) * __ldg(Kb + ((code >> 16) & 255)) *

@@ -465,9 +465,27 @@ __global__ void __launch_bounds__(256) k_prim2(DevCtx ctx, BatchArgs bt, int cp,
 // One group (all image pairs of one set quartet, all contraction rows) processed by NL
 // cooperating lanes (NL = 32: one warp; NL = 1: one lane) whose workspace element x lives at
 // ws[x * ST] (ST = 32 for lane-interleaved per-lane workspaces).
+// The cartesian index tables and the spherical coefficients of the interpreted group kernels,
+// read from a device copy in global memory (DevCtx::gtab, built by build_group_tables): the lanes
+// index them with different values, which the constant cache would serve one address at a time.
+struct GTab {
+   const int8_t *dir, *dec, *inc;
+   const double *c2s;
+};
+
+static __device__ __forceinline__ GTab group_tables(const DevCtx &ctx) {
+   GTab t;
+   t.dir = reinterpret_cast<const int8_t *>(ctx.gtab);
+   t.dec = t.dir + 288;
+   t.inc = t.dir + 1152;
+   t.c2s = reinterpret_cast<const double *>(ctx.gtab + 2016);
+   return t;
+}
+
 template <int NL, int ST>
 static __device__ __forceinline__ void group_body(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan *pl,
-                                                  const GroupRec &G, double *ws, double *cart, int lane) {
+                                                  const GroupRec &G, double *ws, double *cart, int lane,
+                                                  const GTab &tb) {
    const int S = pl->S, Nc = pl->Nc, Ns = pl->Ns;
    const int la = pl->la, lb = pl->lb, lc = pl->lc, ld = pl->ld;
    const int nca = ncart(la), ncb = ncart(lb), ncc = ncart(lc), ncd_ = ncart(ld);
@@ -510,9 +528,9 @@ static __device__ __forceinline__ void group_body(const DevCtx &ctx, const Batch
                   const int nc_ = ncart(c), nd = ncart(d), ncp = ncart(c + 1), ndm = ncart(d - 1);
                   for (int e = lane; e < h.nelem; e += NL) {
                      const int l = e % nd, k = (e / nd) % nc_, ie = e / (nd * nc_);
-                     const int dir = c_cart_dir[d][l];
-                     const int lm = c_cart_dec[d][l][dir];
-                     const int kp = c_cart_inc[c][k][dir];
+                     const int dir = tb.dir[d * 36 + l];
+                     const int lm = tb.dec[(d * 36 + l) * 3 + dir];
+                     const int kp = tb.inc[(c * 36 + k) * 3 + dir];
                      ws[(h.out + e) * ST] = ws[(h.in1 + (ie * ncp + kp) * ndm + lm) * ST] +
                                             CD[dir] * ws[(h.in2 + (ie * nc_ + k) * ndm + lm) * ST];
                   }
@@ -521,9 +539,9 @@ static __device__ __forceinline__ void group_body(const DevCtx &ctx, const Batch
                   const int nb = ncart(b), nbm = ncart(b - 1), cdn = ncc * ncd_;
                   for (int e = lane; e < h.nelem; e += NL) {
                      const int q = e % cdn, j = (e / cdn) % nb, i = e / (cdn * nb);
-                     const int dir = c_cart_dir[b][j];
-                     const int jm = c_cart_dec[b][j][dir];
-                     const int ip = c_cart_inc[a][i][dir];
+                     const int dir = tb.dir[b * 36 + j];
+                     const int jm = tb.dec[(b * 36 + j) * 3 + dir];
+                     const int ip = tb.inc[(a * 36 + i) * 3 + dir];
                      ws[(h.out + e) * ST] = ws[(h.in1 + (ip * nbm + jm) * cdn + q) * ST] +
                                             AB[dir] * ws[(h.in2 + (i * nbm + jm) * cdn + q) * ST];
                   }
@@ -546,7 +564,7 @@ static __device__ __forceinline__ void group_body(const DevCtx &ctx, const Batch
             od[ctr] = ns[ctr];
             const int tot = od[0] * od[1] * od[2] * od[3];
             const int nk = dims[ctr];
-            const double *cc = c_c2s[ls[ctr]];
+            const double *cc = tb.c2s + 70 * ls[ctr];
             int stride = 1;
             for (int q = ctr + 1; q < 4; q++) stride *= dims[q];
             for (int t = lane; t < tot; t += NL) {
@@ -609,6 +627,7 @@ __global__ void __launch_bounds__(256) k_group(DevCtx ctx, BatchArgs bt, int war
    load_plan(bt.plan, smem);
    __syncthreads();
    const int plan_doubles = (int)((sizeof(ClassPlan) + 15) / 16) * 2;
+   const GTab tb = group_tables(ctx);
    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32, nwarp = blockDim.x / 32;
    const int gwarp = blockIdx.x * nwarp + warp;
    double *wbase = use_global ? (bt.gscratch + (size_t)gwarp * warp_doubles)
@@ -616,7 +635,7 @@ __global__ void __launch_bounds__(256) k_group(DevCtx ctx, BatchArgs bt, int war
    const int Hws = max(pl->H, 2 * pl->Nc);
    for (uint32_t g = gwarp; g < bt.ngroup; g += gridDim.x * nwarp) {
       const GroupRec G = bt.groups[g];
-      group_body<32, 1>(ctx, bt, pl, G, wbase, wbase + Hws, lane);
+      group_body<32, 1>(ctx, bt, pl, G, wbase, wbase + Hws, lane, tb);
    }
 }
 
@@ -627,12 +646,13 @@ __global__ void __launch_bounds__(256) k_group_lane(DevCtx ctx, BatchArgs bt, in
    load_plan(bt.plan, smem);
    __syncthreads();
    const int plan_doubles = (int)((sizeof(ClassPlan) + 15) / 16) * 2;
+   const GTab tb = group_tables(ctx);
    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32, nwarp = blockDim.x / 32;
    double *wbase = smem + plan_doubles + (size_t)warp * 32 * lane_doubles + lane;
    const int Hws = max(pl->H, 2 * pl->Nc);
    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < bt.ngroup; g += gridDim.x * blockDim.x) {
       const GroupRec G = bt.groups[g];
-      group_body<1, 32>(ctx, bt, pl, G, wbase, wbase + Hws * 32, 0);
+      group_body<1, 32>(ctx, bt, pl, G, wbase, wbase + Hws * 32, 0, tb);
    }
    (void)nwarp;
 }
@@ -642,6 +662,26 @@ __global__ void __launch_bounds__(256) k_group_lane(DevCtx ctx, BatchArgs bt, in
 // ---------------------------------------------------------------------------------------
 static int h_ncart(int l) { return (l + 1) * (l + 2) / 2; }
 static int h_cidx(int x, int y, int z) { int a = y + z; return a * (a + 1) / 2 + z; }
+
+void build_group_tables(const double *c2s_l0to3, uint8_t *out) {
+   int8_t *dir = reinterpret_cast<int8_t *>(out), *dec = dir + 288, *inc = dir + 1152;
+   for (int i = 0; i < 864; i++) { dec[i] = -1; inc[i] = -1; }
+   for (int l = 0; l < 8; l++) {
+      for (int i = 0; i < h_ncart(l); i++) {
+         int a = 0; while ((a + 1) * (a + 2) / 2 <= i) a++;
+         int e[3]; e[0] = l - a; e[2] = i - a * (a + 1) / 2; e[1] = a - e[2];
+         dir[l * 36 + i] = (int8_t)(e[0] ? 0 : (e[1] ? 1 : 2));
+         for (int q = 0; q < 3; q++) {
+            int f[3] = {e[0], e[1], e[2]};
+            if (f[q] > 0) { f[q]--; dec[(l * 36 + i) * 3 + q] = (int8_t)h_cidx(f[0], f[1], f[2]); }
+            int g[3] = {e[0], e[1], e[2]};
+            g[q]++;
+            if (l + 1 < 8) inc[(l * 36 + i) * 3 + q] = (int8_t)h_cidx(g[0], g[1], g[2]);
+         }
+      }
+   }
+   std::memcpy(out + 2016, c2s_l0to3, sizeof(double) * 4 * 70);
+}
 
 cudaError_t upload_constant_tables(const double *c2s_l0to3, const double *symm5) {
    int8_t exp_[8][36][3] = {}, dir[8][36] = {}, dec[8][36][3], inc[8][36][3];
@@ -770,9 +810,12 @@ size_t group_warp_doubles(const ClassPlan &hp) {
 }
 
 // returns the number of global-scratch doubles needed (0 if the shared-memory path is used)
+// shared memory ahead of the group kernels' workspaces: the class plan
+static size_t group_hdr_bytes() { return (size_t)plan_smem_doubles() * 8; }
+
 size_t group_global_scratch(const ClassPlan &hp, int *grid, int *warps) {
    const size_t wd = group_warp_doubles(hp);
-   const int budget = std::min(max_dyn_smem(), 200 * 1024) - plan_smem_doubles() * 8;
+   const int budget = std::min(max_dyn_smem(), 200 * 1024) - (int)group_hdr_bytes();
    int nw = (int)(budget / (wd * 8));
    if (nw >= 1) return 0;
    *warps = 4;
@@ -798,7 +841,7 @@ cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan
    if (wd <= 40) {
       // small workspace: one lane per group, 32 groups per warp
       const int lane_doubles = (int)wd;
-      const size_t plan_bytes = (size_t)plan_smem_doubles() * 8;
+      const size_t plan_bytes = group_hdr_bytes();
       const int nw = 8;
       const size_t smem = plan_bytes + (size_t)nw * 32 * lane_doubles * 8;
       long blocks = ((long)bt.ngroup + nw * 32 - 1) / (nw * 32);
@@ -806,7 +849,7 @@ cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan
       k_group_lane<<<(unsigned)blocks, nw * 32, smem, st>>>(ctx, bt, lane_doubles);
       return cudaGetLastError();
    }
-   const size_t plan_bytes = (size_t)plan_smem_doubles() * 8;
+   const size_t plan_bytes = group_hdr_bytes();
    const int budget = std::min(max_dyn_smem(), 200 * 1024);
    int nw = (int)((budget - (int)plan_bytes) / (wd * 8));
    if (nw >= 1) {

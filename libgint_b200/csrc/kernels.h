@@ -33,7 +33,12 @@ struct DevCtx {
    int *err;
    unsigned long long *cnt;   // optional event counters per class [256][4], or null
    const VOp *vops;           // precompiled VRR instructions of every class (build_vops)
+   const uint8_t *gtab;       // cartesian index tables and c2s of the group kernels (build_group_tables)
 };
+
+// bytes of the group kernels' table block: direction (8 x 36), decrement and increment
+// (8 x 36 x 3 each) as int8, then the c2s coefficients (4 x 70 doubles)
+constexpr size_t kGroupTabBytes = 288 + 864 + 864 + 4 * 70 * 8;
 
 // One class-sorted segment of a batch (device pointers).
 struct BatchArgs {
@@ -52,6 +57,7 @@ struct BatchArgs {
 bool build_class_plan(int la, int lb, int lc, int ld, ClassPlan &p);
 void build_vops(ClassPlan &p, std::vector<VOp> &out);
 cudaError_t upload_constant_tables(const double *c2s_l0to3, const double *symm5);
+void build_group_tables(const double *c2s_l0to3, uint8_t *out);
 cudaError_t launch_prim(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan &hp, cudaStream_t st);
 cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan &hp, cudaStream_t st);
 size_t group_global_scratch(const ClassPlan &hp, int *grid, int *warps);
