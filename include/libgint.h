@@ -27,6 +27,7 @@
 #define LIBGINT_B200_H
 
 #include <stdbool.h>
+#include <stddef.h>
 
 #ifdef __cplusplus
 extern "C" {
@@ -87,6 +88,19 @@ void libgint_add_qrtt(void *handle, double symm_fac, int la, int lb, int lc, int
 void libgint_add_set(void *handle);
 /* src/extern_functions.cpp:187 launches all queued work */
 void libgint_dispatch(void *handle);
+/* No counterpart in the reference (a bulk form of the call stream above, for callers whose
+ * per-call overhead dominates): the add_prm / add_shell / add_qrt / add_qrtt / add_set calls of n
+ * set quartets in one call, with the same meaning, checks and errors as those calls made in order.
+ * Per set quartet q: sets[4q..4q+3]; shell_count[q] image pairs, each with shell_images (n1, n2)
+ * and prm_count primitive quartets taken in order from prm_codes
+ * (ipa<<24 | ipb<<16 | ipc<<8 | ipd); qrt_count[q] l-combinations, each a record of 8 ints in qrt
+ * (la, lb, lc, ld, nla, nlb, nlc, nld) followed by its nla*nlb*nlc*nld contraction rows in
+ * lexicographic order: qrtt_fac, qrtt_ld (4 ints), qrtt_off (4 unsigned) and qrtt_T (bit 0 Tac,
+ * 1 Tad, 2 Tbc, 3 Tbd). Returns libgint_last_error. */
+int libgint_add_set_quartets(void *handle, int n, const int *sets, const int *shell_count, const int *shell_images,
+                             const int *prm_count, const unsigned int *prm_codes, const int *qrt_count,
+                             const int *qrt, const double *qrtt_fac, const int *qrtt_ld,
+                             const unsigned int *qrtt_off, const unsigned char *qrtt_T);
 
 /* ---- extensions (no counterpart in the reference's C-ABI) ------------------------------- */
 /* last error code of the handle (0 = none); the text is returned by libgint_error_string */

@@ -654,11 +654,15 @@ typedef void (*fn_qrt)(void *, int, int, int, int, int, int, int, int);
 typedef void (*fn_qrtt)(void *, double, int, int, int, int, int, int, int, int, int, int, int, int,
                         unsigned, unsigned, unsigned, unsigned, bool, bool, bool, bool);
 
+typedef int (*fn_bulk)(void *, int, const int *, const int *, const int *, const int *, const unsigned *, const int *,
+                       const int *, const double *, const int *, const unsigned *, const unsigned char *);
+
 struct gd_api {
    void *dl;
    fn_create create; fn_h init; fn_pot pot; fn_d hf; fn_i maxmem; fn_P setP; fn_getK getK;
    fn_cell cell; fn_neighs neighs; fn_atom atom; fn_atomL atomL; fn_prm prm; fn_shell shell;
    fn_qrt qrt; fn_qrtt qrtt; fn_h addset; fn_h dispatch; fn_h destroy;
+   fn_bulk bulk;   // libgint_add_set_quartets, if the library has it
 };
 
 gd_api *gd_api_open(const char *path) {
@@ -686,6 +690,7 @@ gd_api *gd_api_open(const char *path) {
    SYM(dispatch, fn_h, "libgint_dispatch");
 #undef SYM
    a->destroy = (fn_h)dlsym(dl, "libgint_destroy_handle");
+   a->bulk = (fn_bulk)dlsym(dl, "libgint_add_set_quartets");
    return a;
 }
 
@@ -712,8 +717,10 @@ void *gd_setup(const gd_workload *w, gd_api *a, int max_mem_mb) {
 // One K build: set_P, the add_* stream of set quartets [q0, q1), get_K. Returns wall ms.
 // times[0] = set_P, [1] = stream, [2] = get_K (ms). P == nullptr uses the workload's P.
 static double build_K_impl(const gd_workload *w, gd_api *a, void *h, const double *P, double *K,
-                           long q0, long q1, const long *idx, double *times);
+                           long q0, long q1, const long *idx, double *times, bool bulk = false);
 static int g_reverse_prims = 0;
+static int g_bulk = 0;        // stream through libgint_add_set_quartets when the library has it
+void gd_set_bulk(int on) { g_bulk = on; }
 static long g_only_shell = -1;   // replay only this shell (index within its set quartet), -1: all
 void gd_set_only_shell(long k) { g_only_shell = k; }
 // replay the primitive quartets of every shell in reverse order (a reordering of the same sums)
@@ -721,24 +728,106 @@ void gd_set_reverse_prims(int on) { g_reverse_prims = on; }
 
 double gd_build_K(const gd_workload *w, gd_api *a, void *h, const double *P, double *K,
                   long q0, long q1, double *times) {
-   return build_K_impl(w, a, h, P, K, q0, q1, nullptr, times);
+   return build_K_impl(w, a, h, P, K, q0, q1, nullptr, times, g_bulk != 0);
 }
 
 // the same for an explicit list of set quartets idx[0..n)
 double gd_build_K_subset(const gd_workload *w, gd_api *a, void *h, const double *P, double *K,
                          const long *idx, long n, double *times) {
-   return build_K_impl(w, a, h, P, K, 0, n, idx, times);
+   return build_K_impl(w, a, h, P, K, 0, n, idx, times, g_bulk != 0);
+}
+
+// the add_* arguments of one set quartet's contraction rows, in the packed block layout of P/K:
+// the pair (x,y) lands in block (max, min); T selects the transposed walk when x < y; ld =
+// functions of the block's row set (< 256)
+static void qrtt_addr(const gd_workload *w, int sx, int sy, int inx, int iny, unsigned &off, int &ld, bool &T) {
+   const int S = (int)w->sets.size();
+   const SetDef &dx = w->defs[w->sets[sx].def], &dy = w->defs[w->sets[sy].def];
+   int nsx = 2 * dx.l + 1, nsy = 2 * dy.l + 1;
+   if (sx >= sy) {
+      T = false; ld = nsx * dx.nl;
+      off = w->blkoff[(size_t)sx * S + sy] + (unsigned)(iny * nsy * ld + inx * nsx);
+   } else {
+      T = true; ld = nsy * dy.nl;
+      off = w->blkoff[(size_t)sy * S + sx] + (unsigned)(inx * nsx * ld + iny * nsy);
+   }
+}
+
+// The same stream through libgint_add_set_quartets, in chunks of set quartets: the chunk's
+// shells, primitive codes and contraction rows are counted first, then written by index into
+// arrays that keep their capacity from chunk to chunk.
+static void stream_bulk(const gd_workload *w, gd_api *a, void *h, long q0, long q1, const long *idx) {
+   const long CH = 4096;
+   std::vector<int> sets, shc, shi, pc, qc, qr, ld;
+   std::vector<unsigned> codes, off;
+   std::vector<double> fac;
+   std::vector<unsigned char> T;
+   for (long c0 = q0; c0 < q1; c0 += CH) {
+      const long c1 = std::min(q1, c0 + CH), nq = c1 - c0;
+      size_t nsh = 0, npr = 0, nrow = 0;
+      for (long iq0 = c0; iq0 < c1; iq0++) {
+         const SetQ &q = w->setq[idx ? idx[iq0] : iq0];
+         for (uint32_t hs = q.shell_begin; hs < q.shell_end; hs++) {
+            if (g_only_shell >= 0 && (long)(hs - q.shell_begin) != g_only_shell) continue;
+            nsh++;
+            npr += w->shells[hs].prm_end - w->shells[hs].prm_begin;
+         }
+         nrow += (size_t)w->defs[w->sets[q.i].def].nl * w->defs[w->sets[q.j].def].nl *
+                 w->defs[w->sets[q.k].def].nl * w->defs[w->sets[q.l].def].nl;
+      }
+      sets.resize(4 * nq); shc.resize(nq); qc.resize(nq); qr.resize(8 * nq);
+      shi.resize(2 * nsh); pc.resize(nsh); codes.resize(npr);
+      fac.resize(nrow); ld.resize(4 * nrow); off.resize(4 * nrow); T.resize(nrow);
+      size_t ish = 0, ip = 0, ir = 0;
+      for (long iq0 = c0; iq0 < c1; iq0++) {
+         const long k = iq0 - c0;
+         const SetQ &q = w->setq[idx ? idx[iq0] : iq0];
+         const SetDef *d4[4] = {&w->defs[w->sets[q.i].def], &w->defs[w->sets[q.j].def], &w->defs[w->sets[q.k].def],
+                                &w->defs[w->sets[q.l].def]};
+         int *s4 = &sets[4 * k];
+         s4[0] = q.i; s4[1] = q.j; s4[2] = q.k; s4[3] = q.l;
+         int ns = 0;
+         for (uint32_t hs = q.shell_begin; hs < q.shell_end; hs++) {
+            if (g_only_shell >= 0 && (long)(hs - q.shell_begin) != g_only_shell) continue;
+            const Shell &sh = w->shells[hs];
+            shi[2 * ish] = sh.n1; shi[2 * ish + 1] = sh.n2;
+            const int np = (int)(sh.prm_end - sh.prm_begin);
+            pc[ish++] = np;
+            for (int pp = 0; pp < np; pp++)
+               codes[ip++] = w->prims[g_reverse_prims ? sh.prm_end - 1 - pp : sh.prm_begin + pp];
+            ns++;
+         }
+         shc[k] = ns;
+         qc[k] = 1;
+         int *r = &qr[8 * k];
+         r[0] = d4[0]->l; r[1] = d4[1]->l; r[2] = d4[2]->l; r[3] = d4[3]->l;
+         r[4] = d4[0]->nl; r[5] = d4[1]->nl; r[6] = d4[2]->nl; r[7] = d4[3]->nl;
+         for (int ia = 0; ia < d4[0]->nl; ia++) for (int ib = 0; ib < d4[1]->nl; ib++)
+         for (int ic = 0; ic < d4[2]->nl; ic++) for (int id = 0; id < d4[3]->nl; id++, ir++) {
+            bool t4[4];
+            qrtt_addr(w, q.i, q.k, ia, ic, off[4 * ir + 0], ld[4 * ir + 0], t4[0]);
+            qrtt_addr(w, q.i, q.l, ia, id, off[4 * ir + 1], ld[4 * ir + 1], t4[1]);
+            qrtt_addr(w, q.j, q.k, ib, ic, off[4 * ir + 2], ld[4 * ir + 2], t4[2]);
+            qrtt_addr(w, q.j, q.l, ib, id, off[4 * ir + 3], ld[4 * ir + 3], t4[3]);
+            fac[ir] = (double)q.fac;
+            T[ir] = (unsigned char)((t4[0] ? 1 : 0) | (t4[1] ? 2 : 0) | (t4[2] ? 4 : 0) | (t4[3] ? 8 : 0));
+         }
+      }
+      a->bulk(h, (int)nq, sets.data(), shc.data(), shi.data(), pc.data(), codes.data(), qc.data(), qr.data(),
+              fac.data(), ld.data(), off.data(), T.data());
+   }
 }
 
 static double build_K_impl(const gd_workload *w, gd_api *a, void *h, const double *P, double *K,
-                           long q0, long q1, const long *idx, double *times) {
+                           long q0, long q1, const long *idx, double *times, bool bulk) {
    using clk = std::chrono::steady_clock;
    const int S = (int)w->sets.size();
    if (!idx && (q1 < 0 || q1 > (long)w->setq.size())) q1 = (long)w->setq.size();
    auto t0 = clk::now();
    a->setP(h, const_cast<double *>(P ? P : w->Pflat.data()), (int)w->flat_size);
    auto t1 = clk::now();
-   for (long iq0 = q0; iq0 < q1; iq0++) {
+   if (bulk && a->bulk) stream_bulk(w, a, h, q0, q1, idx);
+   else for (long iq0 = q0; iq0 < q1; iq0++) {
       const SetQ &q = w->setq[idx ? idx[iq0] : iq0];
       const Set *s4[4] = {&w->sets[q.i], &w->sets[q.j], &w->sets[q.k], &w->sets[q.l]};
       const SetDef *d4[4] = {&w->defs[s4[0]->def], &w->defs[s4[1]->def], &w->defs[s4[2]->def], &w->defs[s4[3]->def]};
@@ -757,15 +846,7 @@ static double build_K_impl(const gd_workload *w, gd_api *a, void *h, const doubl
       // K/P addressing in the packed block layout: the pair (x,y) lands in block (max, min);
       // T selects the transposed walk when x < y. ld = functions of the block's row set (< 256).
       auto addr = [&](int sx, int sy, int inx, int iny, unsigned &off, int &ld, bool &T) {
-         const SetDef &dx = w->defs[w->sets[sx].def], &dy = w->defs[w->sets[sy].def];
-         int nsx = 2 * dx.l + 1, nsy = 2 * dy.l + 1;
-         if (sx >= sy) {
-            T = false; ld = nsx * dx.nl;
-            off = w->blkoff[(size_t)sx * S + sy] + (unsigned)(iny * nsy * ld + inx * nsx);
-         } else {
-            T = true; ld = nsy * dy.nl;
-            off = w->blkoff[(size_t)sy * S + sx] + (unsigned)(inx * nsx * ld + iny * nsy);
-         }
+         qrtt_addr(w, sx, sy, inx, iny, off, ld, T);
       };
       for (int ia = 0; ia < d4[0]->nl; ia++) for (int ib = 0; ib < d4[1]->nl; ib++)
       for (int ic = 0; ic < d4[2]->nl; ic++) for (int id = 0; id < d4[3]->nl; id++) {
@@ -821,7 +902,7 @@ double gd_build_K_mt(const gd_workload *w, gd_api *a, void **handles, int nh, co
    for (int t = 0; t < nh; t++)
       th.emplace_back([&, t]() {
          Ks[t].assign(w->flat_size, 0.0);
-         tw[t] = build_K_impl(w, a, handles[t], P, Ks[t].data(), cut[t], cut[t + 1], idx, &tt[3 * t]);
+         tw[t] = build_K_impl(w, a, handles[t], P, Ks[t].data(), cut[t], cut[t + 1], idx, &tt[3 * t], g_bulk != 0);
       });
    for (auto &x : th) x.join();
    auto t1 = clk::now();

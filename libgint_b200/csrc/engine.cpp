@@ -1034,6 +1034,45 @@ void libgint_add_set(void *hh) {
    if (h->pend_ac * 8 > budget * 7 / 10 || h->pend_rec > budget * 3 / 10) flush(h);
 }
 
+// The add_prm / add_shell / add_qrt / add_qrtt / add_set stream of n set quartets in one call,
+// processed exactly as those calls made in order (same checks, same errors). Per set quartet q:
+// sets[4q..4q+3]; shell_count[q] image pairs, each with shell_images (n1, n2) and prm_count
+// primitive quartets taken in order from prm_codes (ipa<<24 | ipb<<16 | ipc<<8 | ipd);
+// qrt_count[q] l-combinations, each a qrt record (la, lb, lc, ld, nla, nlb, nlc, nld) followed by
+// its nla*nlb*nlc*nld contraction rows in lexicographic order: qrtt_fac, qrtt_ld (4), qrtt_off (4)
+// and qrtt_T (bit0 Tac, bit1 Tad, bit2 Tbc, bit3 Tbd).
+int libgint_add_set_quartets(void *hh, int n, const int *sets, const int *shell_count, const int *shell_images,
+                             const int *prm_count, const unsigned int *prm_codes, const int *qrt_count,
+                             const int *qrt, const double *qrtt_fac, const int *qrtt_ld,
+                             const unsigned int *qrtt_off, const unsigned char *qrtt_T) {
+   Handle *h = (Handle *)hh;
+   size_t ish = 0, ip = 0, iqrt = 0, ir = 0;
+   for (int q = 0; q < n; q++) {
+      const int *s4 = sets + 4 * (size_t)q;
+      for (int k = 0; k < shell_count[q]; k++, ish++) {
+         const int np = prm_count[ish];
+         h->prm_tmp.assign(prm_codes + ip, prm_codes + ip + np);
+         ip += (size_t)np;
+         libgint_add_shell(h, s4[0], s4[1], s4[2], s4[3], shell_images[2 * ish], shell_images[2 * ish + 1]);
+      }
+      for (int t = 0; t < qrt_count[q]; t++, iqrt++) {
+         const int *r = qrt + 8 * iqrt;
+         libgint_add_qrt(h, r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[7]);
+         const int na = std::max(r[4], 0), nb = std::max(r[5], 0), nc = std::max(r[6], 0), nd = std::max(r[7], 0);
+         for (int ia = 0; ia < na; ia++) for (int ib = 0; ib < nb; ib++)
+         for (int ic = 0; ic < nc; ic++) for (int id = 0; id < nd; id++, ir++) {
+            const int *l4 = qrtt_ld + 4 * ir;
+            const unsigned int *o4 = qrtt_off + 4 * ir;
+            const unsigned char T = qrtt_T[ir];
+            libgint_add_qrtt(h, qrtt_fac[ir], r[0], r[1], r[2], r[3], ia, ib, ic, id, l4[0], l4[1], l4[2], l4[3],
+                             o4[0], o4[1], o4[2], o4[3], (T & 1) != 0, (T & 2) != 0, (T & 4) != 0, (T & 8) != 0);
+         }
+      }
+      libgint_add_set(h);
+   }
+   return h->err;
+}
+
 void libgint_dispatch(void *hh) { flush((Handle *)hh); }
 
 int libgint_last_error(void *hh) { return ((Handle *)hh)->err; }

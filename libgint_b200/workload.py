@@ -80,6 +80,8 @@ def driver():
         lib.gd_mt_split.restype = None
         lib.gd_mt_split.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_long), ctypes.c_long, ctypes.c_int,
                                     ctypes.POINTER(ctypes.c_long)]
+        lib.gd_set_bulk.restype = None
+        lib.gd_set_bulk.argtypes = [ctypes.c_int]
         lib.gd_get_coeffs.restype = ctypes.c_int
         lib.gd_get_coeffs.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D, ctypes.POINTER(ctypes.c_int)]
         lib.gd_teardown.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
@@ -254,3 +256,9 @@ class MultiSession:
             if h:
                 driver().gd_teardown(self.api._a, h)
         self.hs = []
+
+
+def set_bulk(on):
+    """Stream the set quartets through libgint_add_set_quartets (one call per chunk of set
+    quartets) instead of the per-item add_* calls, for libraries that export it."""
+    driver().gd_set_bulk(1 if on else 0)

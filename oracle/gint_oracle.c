@@ -946,6 +946,39 @@ void libgint_add_set(void *hh) {
 
 /* ---- oracle-only controls ---- */
 int libgint_last_error(void *hh) { return ((or_handle*)hh)->error; }
+
+/* The engine's bulk form of the call stream (no reference counterpart): the per-item calls of n
+ * set quartets made in order, so the bulk path of the engine can be checked against the stream. */
+int libgint_add_set_quartets(void *hh, int n, const int *sets, const int *shell_count, const int *shell_images,
+                             const int *prm_count, const unsigned int *prm_codes, const int *qrt_count,
+                             const int *qrt, const double *qrtt_fac, const int *qrtt_ld,
+                             const unsigned int *qrtt_off, const unsigned char *qrtt_T) {
+   size_t ish = 0, ip = 0, iqrt = 0, ir = 0;
+   for (int q = 0; q < n; q++) {
+      const int *s4 = sets + 4 * (size_t)q;
+      for (int k = 0; k < shell_count[q]; k++, ish++) {
+         for (int p = 0; p < prm_count[ish]; p++, ip++) {
+            const unsigned c = prm_codes[ip];
+            libgint_add_prm(hh, (int)(c >> 24), (int)((c >> 16) & 255), (int)((c >> 8) & 255), (int)(c & 255));
+         }
+         libgint_add_shell(hh, s4[0], s4[1], s4[2], s4[3], shell_images[2 * ish], shell_images[2 * ish + 1]);
+      }
+      for (int t = 0; t < qrt_count[q]; t++, iqrt++) {
+         const int *r = qrt + 8 * iqrt;
+         libgint_add_qrt(hh, r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[7]);
+         for (int ia = 0; ia < r[4]; ia++) for (int ib = 0; ib < r[5]; ib++)
+         for (int ic = 0; ic < r[6]; ic++) for (int id = 0; id < r[7]; id++, ir++) {
+            const int *l4 = qrtt_ld + 4 * ir;
+            const unsigned int *o4 = qrtt_off + 4 * ir;
+            const unsigned char T = qrtt_T[ir];
+            libgint_add_qrtt(hh, qrtt_fac[ir], r[0], r[1], r[2], r[3], ia, ib, ic, id, l4[0], l4[1], l4[2], l4[3],
+                             o4[0], o4[1], o4[2], o4[3], (T & 1) != 0, (T & 2) != 0, (T & 4) != 0, (T & 8) != 0);
+         }
+      }
+      libgint_add_set(hh);
+   }
+   return ((or_handle*)hh)->error;
+}
 void oracle_set_threads(void *hh, int n) { ((or_handle*)hh)->nthreads = n; }
 void oracle_destroy(void *hh) {
    or_handle *h = hh;

@@ -149,3 +149,21 @@ def test_multithreaded_caller_matches_oracle(engine_so, oracle_path):
     rel = np.abs(Ke - Ko).max() / np.abs(Ko).max()
     print(f"4 caller threads: engine vs oracle {rel:.3e}, {ms:.1f} ms")
     assert rel <= TOL, rel
+
+
+@pytest.mark.gpu
+def test_bulk_submission_matches_stream(engine_so, oracle_path):
+    """libgint_add_set_quartets (the bulk form of the add_* stream) gives the per-item stream's K."""
+    from libgint_b200.workload import set_bulk
+    wl = Workload("small_l2")
+    Ke, _, code = _k(engine_so, wl)
+    assert code == 0
+    set_bulk(True)
+    try:
+        Kb, _, code_b = _k(engine_so, wl)
+    finally:
+        set_bulk(False)
+    assert code_b == 0
+    rel = np.abs(Kb - Ke).max() / np.abs(Ke).max()
+    print(f"bulk submission vs per-item stream: {rel:.3e}")
+    assert rel <= TOL, rel

@@ -3,7 +3,7 @@ import numpy as np
 import pytest
 
 from conftest import ORACLE_SO
-from libgint_b200.workload import Api, MultiSession, Session, Workload
+from libgint_b200.workload import Api, MultiSession, Session, Workload, set_bulk
 
 
 def test_deterministic():
@@ -104,3 +104,21 @@ def test_multithreaded_caller_sums_to_single_handle():
     K2 = s2.build_K_subset(idx)[0]
     s2.close()
     assert np.abs(Ks - K2).max() <= 1e-13 * np.abs(K2).max()
+
+
+def test_bulk_stream_equals_per_item_stream():
+    """libgint_add_set_quartets carries the same call stream: identical K from the oracle."""
+    import ctypes
+    ora = Api(ORACLE_SO)
+    w = Workload("small_l2")
+    s = Session(ora, w)
+    set_threads = ora.symbol("oracle_set_threads", None, [ctypes.c_void_p, ctypes.c_int])
+    set_threads(s.h, 1)     # one summation order, so the two K agree bit for bit
+    K1 = s.build_K()[0]
+    set_bulk(True)
+    try:
+        K2 = s.build_K()[0]
+    finally:
+        set_bulk(False)
+    s.close()
+    assert np.array_equal(K1, K2)
