@@ -337,6 +337,23 @@ def run_ours(args, world, rank, local):
         if e:
             raise RuntimeError(f"engine error {e}: {lib.libgint_error_string(ctypes.c_void_p(hh)).decode()}")
     h2d = (h2d_total() - h2d0) // max(1, args.steps)
+    # the same through libgint_add_set_quartets (one call per chunk of set quartets)
+    from libgint_b200.workload import set_bulk
+    set_bulk(True)
+    try:
+        msess.build_K(idx=idx)
+        barrier()
+        bulk_ms = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            Kb, _, _ = msess.build_K(idx=idx)
+            Kb = sum_K(Kb)
+            bulk_ms.append((time.perf_counter() - t0) * 1e3)
+        barrier()
+    finally:
+        set_bulk(False)
+    bulk_ms_step = max_over_ranks(float(np.sum(bulk_ms))) / args.steps
+    bulk_dev = float(np.abs(Kb - K).max() / max(1e-300, np.abs(K).max()))
     msess.close()
     e2e_tot = max_over_ranks(float(np.sum(e2e_ms)))
     e2e_ms_step = e2e_tot / args.steps
@@ -362,6 +379,8 @@ def run_ours(args, world, rank, local):
                     "host_threads": args.host_threads,
                     "slowest_thread_ms": float(np.mean([t[3] for t in e2e_parts])),
                     "k_sum_ms": float(np.mean([t[4] for t in e2e_parts]))},
+            "e2e_bulk": {"value": total_shells / (bulk_ms_step / 1e3), "unit": UNIT, "ms_per_step": bulk_ms_step,
+                         "api": "libgint_add_set_quartets", "max_rel_dK_vs_e2e": bulk_dev},
             "gpu_launches": int(launches),
             "roofline": {"bound": "fp64", "kernel": "k_prim (Fm + VRR + image sum)",
                          "achieved": prim_tflops, "peak": peak, "unit": "TFLOP/s",

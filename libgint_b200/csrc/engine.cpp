@@ -1046,9 +1046,87 @@ int libgint_add_set_quartets(void *hh, int n, const int *sets, const int *shell_
                              const int *qrt, const double *qrtt_fac, const int *qrtt_ld,
                              const unsigned int *qrtt_off, const unsigned char *qrtt_T) {
    Handle *h = (Handle *)hh;
+   ensure_ent_base(h);
+   const int nsets = (int)h->sets.size();
    size_t ish = 0, ip = 0, iqrt = 0, ir = 0;
    for (int q = 0; q < n; q++) {
       const int *s4 = sets + 4 * (size_t)q;
+      // Fast path: one l-combination on four single-l sets, every index in range and nothing
+      // pending from earlier per-item calls. Everything is checked before anything is appended,
+      // so the result is the per-item path's; any other set quartet takes the per-item path below.
+      if (qrt_count[q] == 1 && h->nopen == 0 && h->prm_tmp.empty()) {
+         const int *r = qrt + 8 * iqrt;
+         bool ok = true;
+         for (int k = 0; k < 4; k++) ok = ok && (unsigned)s4[k] < (unsigned)nsets && h->fast[s4[k]].nL == 1 &&
+                                           h->fast[s4[k]].l0 == r[k] && r[4 + k] >= 1 && r[4 + k] <= kMaxNl;
+         const int nrow = ok ? r[4] * r[5] * r[6] * r[7] : 0;
+         size_t jp = ip;
+         if (ok) {
+            const Handle::SetFast fa = h->fast[s4[0]], fb = h->fast[s4[1]], fc = h->fast[s4[2]], fd = h->fast[s4[3]];
+            for (int k = 0; k < shell_count[q] && ok; k++) {
+               const size_t sh = ish + k;
+               ok = (unsigned)shell_images[2 * sh] < (unsigned)h->Ng && (unsigned)shell_images[2 * sh + 1] < (unsigned)h->Ng;
+               for (int t = 0; t < prm_count[sh] && ok; t++) {
+                  const uint32_t c = prm_codes[jp + t];
+                  ok = (int)(c >> 24) < fa.np && (int)((c >> 16) & 255u) < fb.np && (int)((c >> 8) & 255u) < fc.np &&
+                       (int)(c & 255u) < fd.np;
+               }
+               jp += (size_t)std::max(prm_count[sh], 0);
+            }
+            for (int t = 0; t < nrow && ok; t++)
+               for (int u = 0; u < 4; u++) ok = ok && qrtt_ld[4 * (ir + t) + u] >= 0 && qrtt_ld[4 * (ir + t) + u] <= 255;
+         }
+         if (ok) {
+            const Handle::SetFast fa = h->fast[s4[0]], fb = h->fast[s4[1]], fc = h->fast[s4[2]], fd = h->fast[s4[3]];
+            const int cl = cls_of(fa.l0, fb.l0, fc.l0, fd.l0);
+            ClassQ &Q = h->q[cl];
+            const uint32_t shell0 = (uint32_t)Q.shells.size(), qrtt0 = (uint32_t)Q.qrtts.size();
+            const size_t prm0 = Q.prm.size();
+            for (int k = 0; k < shell_count[q]; k++, ish++) {
+               const int np = prm_count[ish];
+               if (np > 0) {
+                  ShellRec sr;
+                  sr.ent[0] = (uint32_t)fa.ent; sr.ent[1] = (uint32_t)fb.ent; sr.ent[2] = (uint32_t)fc.ent; sr.ent[3] = (uint32_t)fd.ent;
+                  sr.prm_off = (uint32_t)Q.prm.size();
+                  sr.nprm = (uint32_t)np;
+                  sr.n1 = (uint16_t)shell_images[2 * ish]; sr.n2 = (uint16_t)shell_images[2 * ish + 1];
+                  sr.group = 0;
+                  const uint32_t sid = (uint32_t)Q.shells.size();
+                  Q.prm.append(prm_codes + ip, (size_t)np);
+                  Q.prm_shell.fill((size_t)np, sid);
+                  Q.shells.push_back(sr);
+               }
+               ip += (size_t)std::max(np, 0);
+            }
+            for (int t = 0; t < nrow; t++, ir++) {
+               const double f = qrtt_fac[ir];
+               QrttRec rr;
+               for (int u = 0; u < 4; u++) { rr.off[u] = qrtt_off[4 * ir + u]; rr.ld[u] = (uint8_t)qrtt_ld[4 * ir + u]; }
+               rr.T = (uint8_t)(qrtt_T[ir] & 15);
+               rr.idx_fac = (uint8_t)(f < 0.1 ? 4 : (f < 0.3 ? 3 : (f < 0.75 ? 2 : (f < 1.5 ? 1 : 0))));
+               rr.pad[0] = rr.pad[1] = 0;
+               Q.qrtts.push_back(rr);
+            }
+            iqrt++;
+            const uint32_t nshell = (uint32_t)Q.shells.size() - shell0;
+            if (nshell > 0) {
+               GroupRec g;
+               g.shell_off = shell0; g.nshell = nshell; g.qrtt_off = qrtt0;
+               for (int u = 0; u < 4; u++) g.nl[u] = (uint8_t)r[4 + u];
+               Q.groups.push_back(g);
+               if (!Q.active) { Q.active = true; h->active.push_back(cl); }
+               const size_t added = Q.prm.size() - prm0;
+               h->pend_prims += added;
+               h->pend_ac += added * (size_t)h->plans[cl].S;
+               h->pend_rec += added * 8 + nshell * sizeof(ShellRec) + sizeof(GroupRec) + nrow * sizeof(QrttRec);
+            } else {
+               Q.qrtts.resize(qrtt0);   // nothing to compute: the group rolls back, as in add_set
+            }
+            const size_t budget = slot_budget_bytes(h);
+            if (h->pend_ac * 8 > budget * 7 / 10 || h->pend_rec > budget * 3 / 10) flush(h);
+            continue;
+         }
+      }
       for (int k = 0; k < shell_count[q]; k++, ish++) {
          const int np = prm_count[ish];
          h->prm_tmp.assign(prm_codes + ip, prm_codes + ip + np);
