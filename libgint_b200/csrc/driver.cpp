@@ -740,8 +740,8 @@ double gd_build_K_subset(const gd_workload *w, gd_api *a, void *h, const double 
 // the add_* arguments of one set quartet's contraction rows, in the packed block layout of P/K:
 // the pair (x,y) lands in block (max, min); T selects the transposed walk when x < y; ld =
 // functions of the block's row set (< 256)
-static void qrtt_addr(const gd_workload *w, int sx, int sy, int inx, int iny, unsigned &off, int &ld, bool &T) {
-   const int S = (int)w->sets.size();
+static inline __attribute__((always_inline)) void qrtt_addr(const gd_workload *w, int S, int sx, int sy, int inx,
+                                                             int iny, unsigned &off, int &ld, bool &T) {
    const SetDef &dx = w->defs[w->sets[sx].def], &dy = w->defs[w->sets[sy].def];
    int nsx = 2 * dx.l + 1, nsy = 2 * dy.l + 1;
    if (sx >= sy) {
@@ -758,6 +758,7 @@ static void qrtt_addr(const gd_workload *w, int sx, int sy, int inx, int iny, un
 // arrays that keep their capacity from chunk to chunk.
 static void stream_bulk(const gd_workload *w, gd_api *a, void *h, long q0, long q1, const long *idx) {
    const long CH = 4096;
+   const int S = (int)w->sets.size();
    std::vector<int> sets, shc, shi, pc, qc, qr, ld;
    std::vector<unsigned> codes, off;
    std::vector<double> fac;
@@ -805,10 +806,10 @@ static void stream_bulk(const gd_workload *w, gd_api *a, void *h, long q0, long 
          for (int ia = 0; ia < d4[0]->nl; ia++) for (int ib = 0; ib < d4[1]->nl; ib++)
          for (int ic = 0; ic < d4[2]->nl; ic++) for (int id = 0; id < d4[3]->nl; id++, ir++) {
             bool t4[4];
-            qrtt_addr(w, q.i, q.k, ia, ic, off[4 * ir + 0], ld[4 * ir + 0], t4[0]);
-            qrtt_addr(w, q.i, q.l, ia, id, off[4 * ir + 1], ld[4 * ir + 1], t4[1]);
-            qrtt_addr(w, q.j, q.k, ib, ic, off[4 * ir + 2], ld[4 * ir + 2], t4[2]);
-            qrtt_addr(w, q.j, q.l, ib, id, off[4 * ir + 3], ld[4 * ir + 3], t4[3]);
+            qrtt_addr(w, S, q.i, q.k, ia, ic, off[4 * ir + 0], ld[4 * ir + 0], t4[0]);
+            qrtt_addr(w, S, q.i, q.l, ia, id, off[4 * ir + 1], ld[4 * ir + 1], t4[1]);
+            qrtt_addr(w, S, q.j, q.k, ib, ic, off[4 * ir + 2], ld[4 * ir + 2], t4[2]);
+            qrtt_addr(w, S, q.j, q.l, ib, id, off[4 * ir + 3], ld[4 * ir + 3], t4[3]);
             fac[ir] = (double)q.fac;
             T[ir] = (unsigned char)((t4[0] ? 1 : 0) | (t4[1] ? 2 : 0) | (t4[2] ? 4 : 0) | (t4[3] ? 8 : 0));
          }
@@ -846,7 +847,7 @@ static double build_K_impl(const gd_workload *w, gd_api *a, void *h, const doubl
       // K/P addressing in the packed block layout: the pair (x,y) lands in block (max, min);
       // T selects the transposed walk when x < y. ld = functions of the block's row set (< 256).
       auto addr = [&](int sx, int sy, int inx, int iny, unsigned &off, int &ld, bool &T) {
-         qrtt_addr(w, sx, sy, inx, iny, off, ld, T);
+         qrtt_addr(w, S, sx, sy, inx, iny, off, ld, T);
       };
       for (int ia = 0; ia < d4[0]->nl; ia++) for (int ib = 0; ib < d4[1]->nl; ib++)
       for (int ic = 0; ic < d4[2]->nl; ic++) for (int id = 0; id < d4[3]->nl; id++) {

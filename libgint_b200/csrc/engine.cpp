@@ -255,6 +255,7 @@ struct Handle {
    int nspin = 0;
    size_t FP_size = 0;
    ClassPlan plans[256];
+   int S_of[256];                   // plans[c].S, kept compact for the streaming path
    bool plans_ready = false;
    // streaming state
    std::vector<uint32_t> prm_tmp;
@@ -742,6 +743,7 @@ void *libgint_create_handle(void) {
    for (int c = 0; c < 256; c++) {
       build_class_plan(c >> 6, (c >> 4) & 3, (c >> 2) & 3, c & 3, h->plans[c]);
       build_vops(h->plans[c], h->vops);
+      h->S_of[c] = h->plans[c].S;
    }
    return h;
 }
@@ -1026,7 +1028,7 @@ void libgint_add_set(void *hh) {
       if (!Q.active) { Q.active = true; h->active.push_back(og.cls); }
       const size_t added = Q.prm.size() - og.prm_off;
       h->pend_prims += added;
-      h->pend_ac += added * (size_t)h->plans[og.cls].S;
+      h->pend_ac += added * (size_t)h->S_of[og.cls];
       h->pend_rec += added * 8 + nshell * sizeof(ShellRec) + sizeof(GroupRec) + nrows * sizeof(QrttRec);
    }
    h->nopen = 0;
@@ -1117,7 +1119,7 @@ int libgint_add_set_quartets(void *hh, int n, const int *sets, const int *shell_
                if (!Q.active) { Q.active = true; h->active.push_back(cl); }
                const size_t added = Q.prm.size() - prm0;
                h->pend_prims += added;
-               h->pend_ac += added * (size_t)h->plans[cl].S;
+               h->pend_ac += added * (size_t)h->S_of[cl];
                h->pend_rec += added * 8 + nshell * sizeof(ShellRec) + sizeof(GroupRec) + nrow * sizeof(QrttRec);
             } else {
                Q.qrtts.resize(qrtt0);   // nothing to compute: the group rolls back, as in add_set
