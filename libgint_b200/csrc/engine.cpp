@@ -249,7 +249,7 @@ struct Handle {
    std::vector<SetFast> fast;
    bool basis_dirty = true, ent_dirty = true;
    // device-resident data
-   DBuf d_pool, d_ents, d_neighs, d_C0, d_lut, d_bw, d_ft, d_plans, d_err, d_vops, d_gtab;
+   DBuf d_pool, d_ents, d_neighs, d_C0, d_lut, d_bw, d_ft, d_plans, d_err, d_vops;
    std::vector<VOp> vops;           // precompiled VRR instructions of all classes
    DBuf d_P[2], d_K[2];
    int nspin = 0;
@@ -364,10 +364,6 @@ static bool upload_tables(Handle *h) {
       make_c2s(c2s);
       const double symm[5] = {2.0, 1.0, 0.5, 0.25, 0.0};
       if (!ck(h, upload_constant_tables(&c2s[0][0], symm), "constant tables")) return false;
-      std::vector<uint8_t> gtab(kGroupTabBytes);
-      build_group_tables(&c2s[0][0], gtab.data());
-      if (!ensure(h, h->d_gtab, kGroupTabBytes, "group tables")) return false;
-      if (!h2d(h, h->d_gtab.p, gtab.data(), kGroupTabBytes, "group tables")) return false;
       h->plans_ready = true;
       uploaded = true;
    }
@@ -476,7 +472,7 @@ static DevCtx make_ctx(Handle *h) {
    c.err = (int *)h->d_err.p;
    c.cnt = h->counting ? (unsigned long long *)h->d_cnt.p : nullptr;
    c.vops = (const VOp *)h->d_vops.p;
-   c.gtab = (const uint8_t *)h->d_gtab.p;
+   c.gprog = group_prog(h->device);
    return c;
 }
 
@@ -757,6 +753,7 @@ void libgint_init(void *hh) {
       cudaError_t pe = cudaSuccess;
       std::call_once(loaded[h->device], [&]() { pe = preload_kernels(); });
       ck(h, pe, "kernel preload");
+      if (!h->err && !group_prog(h->device)) set_error(h, 4, "kernel preload: no HRR instructions on this device");
    }
    if (!h->stream) ck(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream");
    for (int w = 0; w < kWorkStreams; w++) {
@@ -1355,7 +1352,7 @@ void libgint_destroy_handle(void *hh) {
    }
    for (auto &rb : h->recs) release(rb.rec);
    release(h->rec_ac); release(h->rec_gscr); release(h->d_cnt);
-   DBuf *bufs[] = {&h->d_pool, &h->d_ents, &h->d_neighs, &h->d_C0, &h->d_lut, &h->d_bw, &h->d_ft, &h->d_vops, &h->d_gtab,
+   DBuf *bufs[] = {&h->d_pool, &h->d_ents, &h->d_neighs, &h->d_C0, &h->d_lut, &h->d_bw, &h->d_ft, &h->d_vops,
                    &h->d_plans, &h->d_err, &h->d_P[0], &h->d_P[1], &h->d_K[0], &h->d_K[1]};
    for (DBuf *b : bufs) release(*b);
    for (int w = 0; w < kWorkStreams; w++) {

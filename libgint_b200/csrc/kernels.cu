@@ -465,27 +465,50 @@ __global__ void __launch_bounds__(256) k_prim2(DevCtx ctx, BatchArgs bt, int cp,
 // One group (all image pairs of one set quartet, all contraction rows) processed by NL
 // cooperating lanes (NL = 32: one warp; NL = 1: one lane) whose workspace element x lives at
 // ws[x * ST] (ST = 32 for lane-interleaved per-lane workspaces).
-// The cartesian index tables and the spherical coefficients of the interpreted group kernels,
-// read from a device copy in global memory (DevCtx::gtab, built by build_group_tables): the lanes
-// index them with different values, which the constant cache would serve one address at a time.
-struct GTab {
-   const int8_t *dir, *dec, *inc;
-   const double *c2s;
-};
-
-static __device__ __forceinline__ GTab group_tables(const DevCtx &ctx) {
-   GTab t;
-   t.dir = reinterpret_cast<const int8_t *>(ctx.gtab);
-   t.dec = t.dir + 288;
-   t.inc = t.dir + 1152;
-   t.c2s = reinterpret_cast<const double *>(ctx.gtab + 2016);
-   return t;
+// Nonzero pattern of the cartesian -> spherical rows (bit k of kC2sMask[l][m]: coefficient k of
+// row m), the integer solid-harmonic rows the coefficients are made from. Terms outside it are
+// exact zeros, so leaving them out changes no sum; upload_constant_tables checks the pattern
+// against the coefficients it uploads.
+__host__ __device__ constexpr uint16_t c2s_mask(int l, int m) {
+   constexpr uint16_t t[4][7] = {{0x1, 0, 0, 0, 0, 0, 0},
+                                 {0x2, 0x4, 0x1, 0, 0, 0, 0},
+                                 {0x02, 0x10, 0x29, 0x04, 0x09, 0, 0},
+                                 {0x042, 0x010, 0x142, 0x284, 0x029, 0x084, 0x009}};
+   return t[l][m];
 }
+
+// One spherical pass over centre LX: the workspace is [npre][ncart(LX)][npost] in, and
+// [npre][2LX+1][npost] out. Each lane transforms whole vectors (one (pre, post) pair at a time),
+// so the coefficients are uniform across the warp. Same sum order as a dense row loop.
+template <int LX, int NL, int ST>
+static __device__ __forceinline__ void sph_pass(const double *src, double *dst, int npre, int npost, int lane) {
+   constexpr int NK = (LX + 1) * (LX + 2) / 2, NSX = 2 * LX + 1;
+   const int nu = npre * npost;
+   for (int u = lane; u < nu; u += NL) {
+      const int pre = u / npost, post = u - pre * npost;
+      const double *s = src + (pre * NK * npost + post) * ST;
+      double *d = dst + (pre * NSX * npost + post) * ST;
+      double x[NK];
+#pragma unroll
+      for (int k = 0; k < NK; k++) x[k] = s[k * npost * ST];
+#pragma unroll
+      for (int m = 0; m < NSX; m++) {
+         double acc = 0.0;
+#pragma unroll
+         for (int k = 0; k < NK; k++)
+            if (c2s_mask(LX, m) >> k & 1) acc += c_c2s[LX][m * NK + k] * x[k];
+         d[m * npost * ST] = acc;
+      }
+   }
+}
+
+// q = t / n for t * n < 2^20, with M = 2^20 / n + 1 (all spherical indices here: t < 7^4, n <= 7^3)
+static __device__ __forceinline__ int div_small(int t, uint32_t M) { return (int)(((uint32_t)t * M) >> 20); }
 
 template <int NL, int ST>
 static __device__ __forceinline__ void group_body(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan *pl,
                                                   const GroupRec &G, double *ws, double *cart, int lane,
-                                                  const GTab &tb) {
+                                                  const uint2 *hrec, double *kpw) {
    const int S = pl->S, Nc = pl->Nc, Ns = pl->Ns;
    const int la = pl->la, lb = pl->lb, lc = pl->lc, ld = pl->ld;
    const int nca = ncart(la), ncb = ncart(lb), ncc = ncart(lc), ncd_ = ncart(ld);
@@ -504,46 +527,73 @@ static __device__ __forceinline__ void group_body(const DevCtx &ctx, const Batch
          const double *Kc = ctx.pool + ec.k_off + ic * ec.np;
          const double *Kd = ctx.pool + ed.k_off + id * ed.np;
          // contraction over primitives (reference src/compute_ECO.cpp:131-212)
-         for (int j = lane; j < S; j += NL) {
-            double a = 0.0;
-            for (uint32_t ip = 0; ip < sh.nprm; ip++) {
-               const uint32_t code = bt.prm[sh.prm_off + ip];
-               const double kp = __ldg(Ka + (code >> 24)) * __ldg(Kb + ((code >> 16) & 255)) *
-                                 __ldg(Kc + ((code >> 8) & 255)) * __ldg(Kd + (code & 255));
-               a += kp * bt.AC[(size_t)(sh.prm_off + ip) * S + j];
+         if constexpr (NL == 32) {
+            // the contraction coefficients of 32 primitives at a time, one per lane, then every
+            // lane sums its targets over them in primitive order
+            if (sh.nprm == 0)
+               for (int j = lane; j < S; j += NL) ws[j] = 0.0;
+            for (uint32_t p0 = 0; p0 < sh.nprm; p0 += 32) {
+               const int np = (int)min(32u, sh.nprm - p0);
+               if (lane < np) {
+                  const uint32_t code = __ldg(bt.prm + sh.prm_off + p0 + lane);
+                  kpw[lane] = __ldg(Ka + (code >> 24)) * __ldg(Kb + ((code >> 16) & 255)) *
+                              __ldg(Kc + ((code >> 8) & 255)) * __ldg(Kd + (code & 255));
+               }
+               __syncwarp();
+               const double *acp = bt.AC + (size_t)(sh.prm_off + p0) * S;
+               for (int j = lane; j < S; j += NL) {
+                  double a = p0 ? ws[j] : 0.0;
+                  const double *rp = acp + j;
+                  int q = 0;
+                  for (; q + 4 <= np; q += 4) {
+                     const double v0 = __ldg(rp), v1 = __ldg(rp + S), v2 = __ldg(rp + 2 * S), v3 = __ldg(rp + 3 * S);
+                     a += kpw[q] * v0;
+                     a += kpw[q + 1] * v1;
+                     a += kpw[q + 2] * v2;
+                     a += kpw[q + 3] * v3;
+                     rp += 4 * S;
+                  }
+                  for (; q < np; q++) { a += kpw[q] * __ldg(rp); rp += S; }
+                  ws[j] = a;
+               }
+               __syncwarp();
             }
-            ws[j * ST] = a;
+         } else {
+            for (int j = lane; j < S; j += NL) {
+               double a = 0.0;
+               for (uint32_t ip = 0; ip < sh.nprm; ip++) {
+                  const uint32_t code = bt.prm[sh.prm_off + ip];
+                  const double kp = __ldg(Ka + (code >> 24)) * __ldg(Kb + ((code >> 16) & 255)) *
+                                    __ldg(Kc + ((code >> 8) & 255)) * __ldg(Kd + (code & 255));
+                  a += kp * bt.AC[(size_t)(sh.prm_off + ip) * S + j];
+               }
+               ws[j * ST] = a;
+            }
          }
          if (NL > 1) __syncwarp();
          double A[3], B[3], C[3], D[3], CDs[3];
          shell_geom(ctx, ea, eb, ec, ed, sh.n1, sh.n2, A, B, C, D, CDs);
-         const double AB[3] = {A[0] - B[0], A[1] - B[1], A[2] - B[2]};
-         const double CD[3] = {C[0] - D[0], C[1] - D[1], C[2] - D[2]};
-         // HRR (reference src/compute_HRR.cpp:7-99)
+         // HRR (reference src/compute_HRR.cpp:7-99), one precompiled instruction per element; the
+         // elements of one level are independent, so each lane loads four before it stores any
          for (int lv = 1; lv <= pl->nhlev; lv++) {
-            for (int o = pl->hlev_off[lv - 1]; o < pl->hlev_off[lv]; o++) {
-               const HOp h = pl->hop[o];
-               if (h.type == 0) {
-                  const int c = h.x, d = h.y;
-                  const int nc_ = ncart(c), nd = ncart(d), ncp = ncart(c + 1), ndm = ncart(d - 1);
-                  for (int e = lane; e < h.nelem; e += NL) {
-                     const int l = e % nd, k = (e / nd) % nc_, ie = e / (nd * nc_);
-                     const int dir = tb.dir[d * 36 + l];
-                     const int lm = tb.dec[(d * 36 + l) * 3 + dir];
-                     const int kp = tb.inc[(c * 36 + k) * 3 + dir];
-                     ws[(h.out + e) * ST] = ws[(h.in1 + (ie * ncp + kp) * ndm + lm) * ST] +
-                                            CD[dir] * ws[(h.in2 + (ie * nc_ + k) * ndm + lm) * ST];
-                  }
-               } else {
-                  const int a = h.x, b = h.y;
-                  const int nb = ncart(b), nbm = ncart(b - 1), cdn = ncc * ncd_;
-                  for (int e = lane; e < h.nelem; e += NL) {
-                     const int q = e % cdn, j = (e / cdn) % nb, i = e / (cdn * nb);
-                     const int dir = tb.dir[b * 36 + j];
-                     const int jm = tb.dec[(b * 36 + j) * 3 + dir];
-                     const int ip = tb.inc[(a * 36 + i) * 3 + dir];
-                     ws[(h.out + e) * ST] = ws[(h.in1 + (ip * nbm + jm) * cdn + q) * ST] +
-                                            AB[dir] * ws[(h.in2 + (i * nbm + jm) * cdn + q) * ST];
+            const HOp h0 = pl->hop[pl->hlev_off[lv - 1]], h1 = pl->hop[pl->hlev_off[lv] - 1];
+            const int x0 = h0.out, x1 = h1.out + h1.nelem;
+            double R0, R1, R2;
+            if (h0.type == 0) { R0 = C[0] - D[0]; R1 = C[1] - D[1]; R2 = C[2] - D[2]; }
+            else { R0 = A[0] - B[0]; R1 = A[1] - B[1]; R2 = A[2] - B[2]; }
+            for (int x = x0 + lane; x < x1; x += 4 * NL) {
+               uint2 ins[4];
+#pragma unroll
+               for (int u = 0; u < 4; u++) ins[u] = __ldg(&hrec[min(x + u * NL, x1 - 1) - S]);
+               double w1[4], w2[4];
+#pragma unroll
+               for (int u = 0; u < 4; u++) { w1[u] = ws[(ins[u].x & 0x3fffffffu) * ST]; w2[u] = ws[ins[u].y * ST]; }
+#pragma unroll
+               for (int u = 0; u < 4; u++) {
+                  if (x + u * NL < x1) {
+                     const uint32_t dir = ins[u].x >> 30;
+                     const double Rd = dir == 0 ? R0 : (dir == 1 ? R1 : R2);
+                     ws[(x + u * NL) * ST] = w1[u] + Rd * w2[u];
                   }
                }
             }
@@ -552,43 +602,38 @@ static __device__ __forceinline__ void group_body(const DevCtx &ctx, const Batch
          for (int q = lane; q < Nc; q += NL) cart[q * ST] += ws[(pl->out_off + q) * ST];
          if (NL > 1) __syncwarp();
       }
-      // cartesian -> spherical, one centre at a time (a, b, c, d)
+      // cartesian -> spherical, one centre at a time (a, b, c, d); the two halves of the
+      // workspace take turns as the output, and l = 0 centres (a coefficient of 1) are skipped
+      const double *sph = cart;
       {
          int dims[4] = {nca, ncb, ncc, ncd_};
          const int ls[4] = {la, lb, lc, ld};
          const int ns[4] = {nsa, nsb, nsc, nsd};
-         const double *src = cart;
          for (int ctr = 0; ctr < 4; ctr++) {
-            double *dst = ws + ((ctr & 1) ? Nc * ST : 0);
-            int od[4] = {dims[0], dims[1], dims[2], dims[3]};
-            od[ctr] = ns[ctr];
-            const int tot = od[0] * od[1] * od[2] * od[3];
-            const int nk = dims[ctr];
-            const double *cc = tb.c2s + 70 * ls[ctr];
-            int stride = 1;
-            for (int q = ctr + 1; q < 4; q++) stride *= dims[q];
-            for (int t = lane; t < tot; t += NL) {
-               int rem = t, id4[4];
-               for (int q = 3; q >= 0; q--) { id4[q] = rem % od[q]; rem /= od[q]; }
-               const int mi = id4[ctr];
-               id4[ctr] = 0;
-               const int base = ((id4[0] * dims[1] + id4[1]) * dims[2] + id4[2]) * dims[3] + id4[3];
-               double acc = 0.0;
-               for (int k = 0; k < nk; k++) acc += cc[mi * nk + k] * src[(base + k * stride) * ST];
-               dst[t * ST] = acc;
-            }
+            if (ls[ctr] == 0) continue;
+            double *dst = (sph == ws) ? ws + Nc * ST : ws;
+            int npre = 1, npost = 1;
+            for (int q = 0; q < ctr; q++) npre *= dims[q];
+            for (int q = ctr + 1; q < 4; q++) npost *= dims[q];
+            if (ls[ctr] == 1) sph_pass<1, NL, ST>(sph, dst, npre, npost, lane);
+            else if (ls[ctr] == 2) sph_pass<2, NL, ST>(sph, dst, npre, npost, lane);
+            else sph_pass<3, NL, ST>(sph, dst, npre, npost, lane);
             if (NL > 1) __syncwarp();
             dims[ctr] = ns[ctr];
-            src = dst;
+            sph = dst;
          }
       }
-      const double *sph = ws + Nc * ST;   // after 4 passes the result sits in the odd buffer
       // K update (reference src/compute_KS.cpp:26-115)
       const QrttRec k = bt.qrtts[G.qrtt_off + r];
       const double fac = c_symm[k.idx_fac] * ctx.hf_fac;
       const int nscd = nsc * nsd, nsbcd = nsb * nscd;
+      const uint32_t Mbcd = (1u << 20) / nsbcd + 1, Mcd = (1u << 20) / nscd + 1, Md = (1u << 20) / nsd + 1;
       for (int t = lane; t < Ns; t += NL) {
-         const int isa = t / nsbcd, isb = (t / nscd) % nsb, isc = (t / nsd) % nsc, isd = t % nsd;
+         const int isa = div_small(t, Mbcd);
+         int rem = t - isa * nsbcd;
+         const int isb = div_small(rem, Mcd);
+         rem -= isb * nscd;
+         const int isc = div_small(rem, Md), isd = rem - isc * nsd;
          const int iac = !(k.T & 1) ? isc * k.ld[0] + isa : isa * k.ld[0] + isc;
          const int iad = !(k.T & 2) ? isd * k.ld[1] + isa : isa * k.ld[1] + isd;
          const int ibc = !(k.T & 4) ? isc * k.ld[2] + isb : isb * k.ld[2] + isc;
@@ -627,15 +672,17 @@ __global__ void __launch_bounds__(256) k_group(DevCtx ctx, BatchArgs bt, int war
    load_plan(bt.plan, smem);
    __syncthreads();
    const int plan_doubles = (int)((sizeof(ClassPlan) + 15) / 16) * 2;
-   const GTab tb = group_tables(ctx);
    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32, nwarp = blockDim.x / 32;
    const int gwarp = blockIdx.x * nwarp + warp;
+   // shared memory: plan | nwarp coefficient buffers | nwarp workspaces (unless in global memory)
+   double *kpw = smem + plan_doubles + warp * kGroupKpDoubles;
    double *wbase = use_global ? (bt.gscratch + (size_t)gwarp * warp_doubles)
-                              : (smem + plan_doubles + (size_t)warp * warp_doubles);
+                              : (smem + plan_doubles + nwarp * kGroupKpDoubles + (size_t)warp * warp_doubles);
    const int Hws = max(pl->H, 2 * pl->Nc);
+   const uint2 *hrec = ctx.gprog + ctx.gprog[bt.cls].x;
    for (uint32_t g = gwarp; g < bt.ngroup; g += gridDim.x * nwarp) {
       const GroupRec G = bt.groups[g];
-      group_body<32, 1>(ctx, bt, pl, G, wbase, wbase + Hws, lane, tb);
+      group_body<32, 1>(ctx, bt, pl, G, wbase, wbase + Hws, lane, hrec, kpw);
    }
 }
 
@@ -646,13 +693,13 @@ __global__ void __launch_bounds__(256) k_group_lane(DevCtx ctx, BatchArgs bt, in
    load_plan(bt.plan, smem);
    __syncthreads();
    const int plan_doubles = (int)((sizeof(ClassPlan) + 15) / 16) * 2;
-   const GTab tb = group_tables(ctx);
    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32, nwarp = blockDim.x / 32;
    double *wbase = smem + plan_doubles + (size_t)warp * 32 * lane_doubles + lane;
    const int Hws = max(pl->H, 2 * pl->Nc);
+   const uint2 *hrec = ctx.gprog + ctx.gprog[bt.cls].x;
    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < bt.ngroup; g += gridDim.x * blockDim.x) {
       const GroupRec G = bt.groups[g];
-      group_body<1, 32>(ctx, bt, pl, G, wbase, wbase + Hws * 32, 0, tb);
+      group_body<1, 32>(ctx, bt, pl, G, wbase, wbase + Hws * 32, 0, hrec, nullptr);
    }
    (void)nwarp;
 }
@@ -663,49 +710,90 @@ __global__ void __launch_bounds__(256) k_group_lane(DevCtx ctx, BatchArgs bt, in
 static int h_ncart(int l) { return (l + 1) * (l + 2) / 2; }
 static int h_cidx(int x, int y, int z) { int a = y + z; return a * (a + 1) / 2 + z; }
 
-void build_group_tables(const double *c2s_l0to3, uint8_t *out) {
-   int8_t *dir = reinterpret_cast<int8_t *>(out), *dec = dir + 288, *inc = dir + 1152;
-   for (int i = 0; i < 864; i++) { dec[i] = -1; inc[i] = -1; }
+// Cartesian index tables for l < 8: exponents, the first axis with a nonzero exponent, and the
+// index of the function one lower / one higher on each axis (-1 where that does not exist).
+struct CartTables {
+   int8_t exp_[8][36][3], dir[8][36], dec[8][36][3], inc[8][36][3];
+};
+
+static void make_cart_tables(CartTables &t) {
+   std::memset(&t, 0, sizeof(t));
+   for (int l = 0; l < 8; l++) for (int i = 0; i < 36; i++) for (int q = 0; q < 3; q++) { t.dec[l][i][q] = -1; t.inc[l][i][q] = -1; }
    for (int l = 0; l < 8; l++) {
       for (int i = 0; i < h_ncart(l); i++) {
          int a = 0; while ((a + 1) * (a + 2) / 2 <= i) a++;
          int e[3]; e[0] = l - a; e[2] = i - a * (a + 1) / 2; e[1] = a - e[2];
-         dir[l * 36 + i] = (int8_t)(e[0] ? 0 : (e[1] ? 1 : 2));
+         for (int q = 0; q < 3; q++) t.exp_[l][i][q] = (int8_t)e[q];
+         t.dir[l][i] = (int8_t)(e[0] ? 0 : (e[1] ? 1 : 2));
          for (int q = 0; q < 3; q++) {
             int f[3] = {e[0], e[1], e[2]};
-            if (f[q] > 0) { f[q]--; dec[(l * 36 + i) * 3 + q] = (int8_t)h_cidx(f[0], f[1], f[2]); }
+            if (f[q] > 0) { f[q]--; t.dec[l][i][q] = (int8_t)h_cidx(f[0], f[1], f[2]); }
             int g[3] = {e[0], e[1], e[2]};
             g[q]++;
-            if (l + 1 < 8) inc[(l * 36 + i) * 3 + q] = (int8_t)h_cidx(g[0], g[1], g[2]);
+            if (l + 1 < 8) t.inc[l][i][q] = (int8_t)h_cidx(g[0], g[1], g[2]);
          }
       }
    }
-   std::memcpy(out + 2016, c2s_l0to3, sizeof(double) * 4 * 70);
+}
+
+// The HRR instructions of all 256 classes (layout in kernels.h). Element e of a ket step (c, d)
+// is (ie, k, l) = (e / (nc nd), e / nd % nc, e % nd) and reads (ie, k + 1_t, l - 1_t) and
+// (ie, k, l - 1_t); element e of a bra step (a, b) is (i, j, q) and reads (i + 1_t, j - 1_t, q)
+// and (i, j - 1_t, q), t the first axis on which l (or j) has a nonzero exponent (reference
+// src/compute_HRR.cpp:7-99). The steps' outputs are laid out back to back from S, so element x
+// of the workspace is instruction x - S.
+void build_group_prog(std::vector<uint2> &out) {
+   CartTables t;
+   make_cart_tables(t);
+   out.assign(256, make_uint2(0u, 0u));
+   for (int c = 0; c < 256; c++) {
+      ClassPlan p;
+      out[c].x = (uint32_t)out.size();
+      if (!build_class_plan(c >> 6, (c >> 4) & 3, (c >> 2) & 3, c & 3, p)) continue;
+      int x = p.S;
+      for (int o = 0; o < p.nhop; o++) {
+         const HOp &h = p.hop[o];
+         if (h.out != x) { out.clear(); return; }   // steps not back to back: no program
+         if (h.type == 0) {
+            const int cc = h.x, d = h.y, nc = h_ncart(cc), nd = h_ncart(d), ncp = h_ncart(cc + 1), ndm = h_ncart(d - 1);
+            for (int e = 0; e < h.nelem; e++) {
+               const int l = e % nd, k = (e / nd) % nc, ie = e / (nd * nc);
+               const int dr = t.dir[d][l], lm = t.dec[d][l][dr], kp = t.inc[cc][k][dr];
+               const uint32_t in1 = (uint32_t)(h.in1 + (ie * ncp + kp) * ndm + lm);
+               const uint32_t in2 = (uint32_t)(h.in2 + (ie * nc + k) * ndm + lm);
+               out.push_back(make_uint2(in1 | ((uint32_t)dr << 30), in2));
+            }
+         } else {
+            const int a = h.x, b = h.y, nb = h_ncart(b), nbm = h_ncart(b - 1);
+            const int cdn = h_ncart(p.lc) * h_ncart(p.ld);
+            for (int e = 0; e < h.nelem; e++) {
+               const int q = e % cdn, j = (e / cdn) % nb, i = e / (cdn * nb);
+               const int dr = t.dir[b][j], jm = t.dec[b][j][dr], ip = t.inc[a][i][dr];
+               const uint32_t in1 = (uint32_t)(h.in1 + (ip * nbm + jm) * cdn + q);
+               const uint32_t in2 = (uint32_t)(h.in2 + (i * nbm + jm) * cdn + q);
+               out.push_back(make_uint2(in1 | ((uint32_t)dr << 30), in2));
+            }
+         }
+         x += h.nelem;
+      }
+   }
 }
 
 cudaError_t upload_constant_tables(const double *c2s_l0to3, const double *symm5) {
-   int8_t exp_[8][36][3] = {}, dir[8][36] = {}, dec[8][36][3], inc[8][36][3];
-   for (int l = 0; l < 8; l++) for (int i = 0; i < 36; i++) for (int q = 0; q < 3; q++) { dec[l][i][q] = -1; inc[l][i][q] = -1; }
-   for (int l = 0; l < 8; l++) {
-      for (int i = 0; i < h_ncart(l); i++) {
-         int a = 0; while ((a + 1) * (a + 2) / 2 <= i) a++;
-         int e[3]; e[0] = l - a; e[2] = i - a * (a + 1) / 2; e[1] = a - e[2];
-         for (int q = 0; q < 3; q++) exp_[l][i][q] = (int8_t)e[q];
-         dir[l][i] = (int8_t)(e[0] ? 0 : (e[1] ? 1 : 2));
-         for (int q = 0; q < 3; q++) {
-            int f[3] = {e[0], e[1], e[2]};
-            if (f[q] > 0) { f[q]--; dec[l][i][q] = (int8_t)h_cidx(f[0], f[1], f[2]); }
-            int g[3] = {e[0], e[1], e[2]};
-            g[q]++;
-            if (l + 1 < 8) inc[l][i][q] = (int8_t)h_cidx(g[0], g[1], g[2]);
-         }
-      }
+   // the spherical passes leave out the terms outside the rows' nonzero pattern (c2s_mask)
+   for (int l = 0; l <= 3; l++) {
+      const int nk = h_ncart(l);
+      for (int m = 0; m < 2 * l + 1; m++)
+         for (int k = 0; k < nk; k++)
+            if (((c2s_mask(l, m) >> k & 1) != 0) != (c2s_l0to3[l * 70 + m * nk + k] != 0.0)) return cudaErrorInvalidValue;
    }
+   CartTables t;
+   make_cart_tables(t);
    cudaError_t err;
-   if ((err = cudaMemcpyToSymbol(c_cart_exp, exp_, sizeof(exp_))) != cudaSuccess) return err;
-   if ((err = cudaMemcpyToSymbol(c_cart_dir, dir, sizeof(dir))) != cudaSuccess) return err;
-   if ((err = cudaMemcpyToSymbol(c_cart_dec, dec, sizeof(dec))) != cudaSuccess) return err;
-   if ((err = cudaMemcpyToSymbol(c_cart_inc, inc, sizeof(inc))) != cudaSuccess) return err;
+   if ((err = cudaMemcpyToSymbol(c_cart_exp, t.exp_, sizeof(t.exp_))) != cudaSuccess) return err;
+   if ((err = cudaMemcpyToSymbol(c_cart_dir, t.dir, sizeof(t.dir))) != cudaSuccess) return err;
+   if ((err = cudaMemcpyToSymbol(c_cart_dec, t.dec, sizeof(t.dec))) != cudaSuccess) return err;
+   if ((err = cudaMemcpyToSymbol(c_cart_inc, t.inc, sizeof(t.inc))) != cudaSuccess) return err;
    if ((err = cudaMemcpyToSymbol(c_c2s, c2s_l0to3, sizeof(double) * 4 * 70)) != cudaSuccess) return err;
    return cudaMemcpyToSymbol(c_symm, symm5, sizeof(double) * 5);
 }
@@ -813,11 +901,15 @@ size_t group_warp_doubles(const ClassPlan &hp) {
 // shared memory ahead of the group kernels' workspaces: the class plan
 static size_t group_hdr_bytes() { return (size_t)plan_smem_doubles() * 8; }
 
+// warps per block of k_group with the workspaces in shared memory (0: they do not fit)
+static int group_smem_warps(size_t wd) {
+   const int budget = std::min(max_dyn_smem(), 200 * 1024) - (int)group_hdr_bytes();
+   return std::min(8, (int)(budget / ((wd + kGroupKpDoubles) * 8)));
+}
+
 size_t group_global_scratch(const ClassPlan &hp, int *grid, int *warps) {
    const size_t wd = group_warp_doubles(hp);
-   const int budget = std::min(max_dyn_smem(), 200 * 1024) - (int)group_hdr_bytes();
-   int nw = (int)(budget / (wd * 8));
-   if (nw >= 1) return 0;
+   if (group_smem_warps(wd) >= 1) return 0;
    *warps = 4;
    *grid = 148 * 2;
    return wd * (size_t)(*warps) * (*grid);
@@ -850,18 +942,17 @@ cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan
       return cudaGetLastError();
    }
    const size_t plan_bytes = group_hdr_bytes();
-   const int budget = std::min(max_dyn_smem(), 200 * 1024);
-   int nw = (int)((budget - (int)plan_bytes) / (wd * 8));
+   const int nw = group_smem_warps(wd);
    if (nw >= 1) {
-      nw = std::min(nw, 8);
-      const size_t smem = plan_bytes + (size_t)nw * wd * 8;
+      const size_t smem = plan_bytes + (size_t)nw * (wd + kGroupKpDoubles) * 8;
       long blocks = ((long)bt.ngroup + nw - 1) / nw;
       blocks = std::max(1L, std::min(blocks, 148L * 64));
       k_group<<<(unsigned)blocks, nw * 32, smem, st>>>(ctx, bt, (int)wd, 0);
    } else {
       int grid = 0, warps = 0;
       group_global_scratch(hp, &grid, &warps);
-      k_group<<<grid, warps * 32, plan_bytes, st>>>(ctx, bt, (int)wd, 1);
+      const size_t smem = plan_bytes + (size_t)warps * kGroupKpDoubles * 8;
+      k_group<<<grid, warps * 32, smem, st>>>(ctx, bt, (int)wd, 1);
    }
    return cudaGetLastError();
 }
@@ -906,6 +997,33 @@ double measure_fp64_peak_tflops() {
    return flops / (best * 1e-3) / 1e12;
 }
 
+// The per-device copies of the HRR instructions (build_group_prog), made once per device by
+// preload_kernels and kept until the process exits.
+static const uint2 *g_group_prog[kMaxDevices] = {nullptr};
+
+static cudaError_t group_prog_load() {
+   int dev = 0;
+   cudaError_t e = cudaGetDevice(&dev);
+   if (e != cudaSuccess) return e;
+   if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+   if (g_group_prog[dev]) return cudaSuccess;
+   std::vector<uint2> prog;
+   build_group_prog(prog);
+   if (prog.empty()) return cudaErrorInvalidValue;
+   void *p = nullptr;
+   if ((e = cudaMalloc(&p, prog.size() * sizeof(uint2))) != cudaSuccess) return e;
+   if ((e = cudaMemcpy(p, prog.data(), prog.size() * sizeof(uint2), cudaMemcpyHostToDevice)) != cudaSuccess) {
+      cudaFree(p);
+      return e;
+   }
+   g_group_prog[dev] = (const uint2 *)p;
+   return cudaSuccess;
+}
+
+const uint2 *group_prog(int device) {
+   return (device >= 0 && device < kMaxDevices) ? g_group_prog[device] : nullptr;
+}
+
 // Loads every kernel of the engine on the current device and lets each take up to the device's
 // opt-in shared memory per block. The shared-memory limit is a process-wide attribute of a
 // kernel: set per launch (with the launch's own size), one caller thread could lower it between
@@ -922,7 +1040,8 @@ cudaError_t preload_kernels() {
    cudaFuncAttributes a;
    if ((e = cudaFuncGetAttributes(&a, (const void *)k_fp64_fma)) != cudaSuccess) return e;
    if ((e = prim3_preload(smax)) != cudaSuccess) return e;
-   return group3_preload();
+   if ((e = group3_preload()) != cudaSuccess) return e;
+   return group_prog_load();
 }
 
 // ---------------------------------------------------------------------------------------

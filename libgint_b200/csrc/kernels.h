@@ -33,12 +33,16 @@ struct DevCtx {
    int *err;
    unsigned long long *cnt;   // optional event counters per class [256][4], or null
    const VOp *vops;           // precompiled VRR instructions of every class (build_vops)
-   const uint8_t *gtab;       // cartesian index tables and c2s of the group kernels (build_group_tables)
+   const uint2 *gprog;        // HRR instructions of every class (group_prog), shared by all handles
 };
 
-// bytes of the group kernels' table block: direction (8 x 36), decrement and increment
-// (8 x 36 x 3 each) as int8, then the c2s coefficients (4 x 70 doubles)
-constexpr size_t kGroupTabBytes = 288 + 864 + 864 + 4 * 70 * 8;
+// HRR instructions of the interpreted group kernels, one device copy per GPU (built by
+// preload_kernels). Entries 0..255 hold, in .x, the index of each class's first instruction;
+// instruction cls_first + (x - S) computes HRR workspace element x of that class (S <= x < H):
+//    w[x] = w[in1] + R[dir] * w[in2],   stored as {in1 | dir << 30, in2}
+// with R = CD on the ket levels and AB on the bra levels. Returns null before preload_kernels.
+const uint2 *group_prog(int device);
+void build_group_prog(std::vector<uint2> &out);
 
 // One class-sorted segment of a batch (device pointers).
 struct BatchArgs {
@@ -57,10 +61,10 @@ struct BatchArgs {
 bool build_class_plan(int la, int lb, int lc, int ld, ClassPlan &p);
 void build_vops(ClassPlan &p, std::vector<VOp> &out);
 cudaError_t upload_constant_tables(const double *c2s_l0to3, const double *symm5);
-void build_group_tables(const double *c2s_l0to3, uint8_t *out);
 cudaError_t launch_prim(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan &hp, cudaStream_t st);
 cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan &hp, cudaStream_t st);
 size_t group_global_scratch(const ClassPlan &hp, int *grid, int *warps);
+constexpr int kGroupKpDoubles = 32;   // per-warp shared buffer of contraction coefficients in k_group
 int prim_team_size(const ClassPlan &hp);
 // Fixed device scratch (file-scope device array in kernels.cu) used by libgint_replay_noalloc:
 // its device address for the current device; the first call on a device looks it up.
