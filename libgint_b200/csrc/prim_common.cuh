@@ -101,7 +101,6 @@ static __device__ __forceinline__ void shell_geom(const DevCtx &ctx, const Basis
    }
 }
 
-// Per-primitive-quartet quantities shared by every image n3.
 // Per-primitive-quartet quantities shared by every image n3. D = P - Q is rounded as the
 // reference's T formula rounds it; upper, lower, X2 and i2 (the truncation bounds and the
 // second patch coordinate, which depend on R only) are evaluated exactly as t_c_g0_n does.
