@@ -94,10 +94,6 @@ static __device__ __forceinline__ void vrr_elem_s(const VBlock &b, int e, double
    ws[(b.off + e) * ST] = v;
 }
 
-static __device__ __forceinline__ void vrr_elem(const VBlock &b, int e, double *ws, const double *pqz) {
-   vrr_elem_s<1>(b, e, ws, pqz);
-}
-
 // One level of the precompiled VRR (VOp, see build_vops): instructions [e0, e1) spread over the
 // lanes of a team; ws holds a zero at offset V.
 static __device__ __forceinline__ void vops_level(const VOp *__restrict__ vop, int e0, int e1, int lane, int stride,
@@ -254,7 +250,7 @@ __global__ void __launch_bounds__(256) k_prim2(DevCtx ctx, BatchArgs bt, int cp,
    const int plan_doubles = (int)((sizeof(ClassPlan) + 15) / 16) * 2;
    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
    double *wb = smem + plan_doubles + (size_t)warp * warp_doubles;
-   const int L = pl->L, V = pl->V, S = pl->S, Ng = ctx.Ng;
+   const int L = pl->L, S = pl->S, Ng = ctx.Ng;
    const int LF = L + 1;
    // per-warp layout
    PrimGeo *geo = reinterpret_cast<PrimGeo *>(wb);                     // [cp]
