@@ -230,6 +230,7 @@ struct Handle {
    cudaStream_t work[kWorkStreams] = {};
    cudaEvent_t work_ev[kWorkStreams] = {};
    cudaEvent_t fork_ev = nullptr;
+   cudaEvent_t batch_ev[2][kWorkStreams] = {};   // replay: each worker's end of the last batch of each parity
    int err = 0;
    std::string errmsg;
    // potential and tables
@@ -658,7 +659,12 @@ static double replay_impl(Handle *h, double *kt, double *kcls = nullptr) {
       ac = std::max(ac, rb.ac_doubles);
       for (auto &g : rb.segs) { int a, b; gs = std::max(gs, group_global_scratch(h->plans[g.c], &a, &b)); }
    }
-   if (!ensure(h, h->rec_ac, std::max<size_t>(ac * 8, 256), "replay AC")) return -1.0;
+   // Every batch numbers its AC rows from 0, and the worker streams run the segments of
+   // consecutive batches at the same time, so batches alternate between two halves of the replay
+   // AC buffer (as the streamed build alternates two slots), and batch b + 2, which reuses batch b's
+   // half, starts on each worker only after every worker has finished batch b.
+   ac = (ac + 3) & ~(size_t)3;
+   if (!ensure(h, h->rec_ac, std::max<size_t>(2 * ac * 8, 256), "replay AC")) return -1.0;
    if (gs && !ensure(h, h->rec_gscr, gs * 8, "replay HRR scratch")) return -1.0;
    cudaEvent_t e0, e1;
    cudaEventCreate(&e0); cudaEventCreate(&e1);
@@ -677,8 +683,14 @@ static double replay_impl(Handle *h, double *kt, double *kcls = nullptr) {
    const bool spread = kt == nullptr;
    if (spread) fork_workers(h);
    int nseg = 0;
-   for (auto &rb : h->recs) {
+   for (size_t bi = 0; bi < h->recs.size(); bi++) {
+      auto &rb = h->recs[bi];
       char *base = (char *)rb.rec.p;
+      double *ac_half = (double *)h->rec_ac.p + (bi & 1) * ac;
+      if (spread && bi >= 2)
+         for (int w = 0; w < kWorkStreams; w++)
+            for (int w2 = 0; w2 < kWorkStreams; w2++)
+               ck(h, cudaStreamWaitEvent(h->work[w], h->batch_ev[bi & 1][w2], 0), "stream wait");
       for (auto &g : rb.segs) {
          BatchArgs bt;
          std::memset(&bt, 0, sizeof(bt));
@@ -690,7 +702,7 @@ static double replay_impl(Handle *h, double *kt, double *kcls = nullptr) {
          bt.groups = (const GroupRec *)(base + g.o_g);
          bt.qrtts = (const QrttRec *)(base + g.o_q);
          bt.nprm = g.nprm; bt.nshell = g.nshell; bt.ngroup = g.ngroup;
-         bt.AC = (double *)h->rec_ac.p + g.ac_off;
+         bt.AC = ac_half + g.ac_off;
          bt.gscratch = (double *)h->rec_gscr.p;
          int a_, b_;
          cudaStream_t st = spread ? worker_for(h, nseg++, group_global_scratch(h->plans[g.c], &a_, &b_) != 0)
@@ -703,6 +715,9 @@ static double replay_impl(Handle *h, double *kt, double *kcls = nullptr) {
          kmark();
          h->n_launch += 2;
       }
+      if (spread)
+         for (int w = 0; w < kWorkStreams; w++)
+            ck(h, cudaEventRecord(h->batch_ev[bi & 1][w], h->work[w]), "event record");
    }
    if (spread) join_workers(h);
    ck(h, cudaEventRecord(e1, h->stream), "event");
@@ -763,6 +778,9 @@ void libgint_init(void *hh) {
       if (!h->work_ev[w]) ck(h, cudaEventCreateWithFlags(&h->work_ev[w], cudaEventDisableTiming), "event");
    }
    if (!h->fork_ev) ck(h, cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming), "event");
+   for (auto &row : h->batch_ev)
+      for (cudaEvent_t &e : row)
+         if (!e) ck(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
    for (Slot &s : h->slots) {
       if (!s.ev) ck(h, cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming), "event");
       if (!s.ev_copy) ck(h, cudaEventCreateWithFlags(&s.ev_copy, cudaEventDisableTiming), "event");
@@ -1362,6 +1380,9 @@ void libgint_destroy_handle(void *hh) {
       if (h->work_ev[w]) cudaEventDestroy(h->work_ev[w]);
    }
    if (h->fork_ev) cudaEventDestroy(h->fork_ev);
+   for (auto &row : h->batch_ev)
+      for (cudaEvent_t e : row)
+         if (e) cudaEventDestroy(e);
    if (h->stream) cudaStreamDestroy(h->stream);
    delete h;
 }

@@ -110,6 +110,33 @@ def test_record_replay_matches_stream(engine_so):
 
 
 @pytest.mark.gpu
+def test_multi_batch_replay_matches_stream(engine_so):
+    """A recording of many batches replays to the streamed K, twice in a row. The worker streams
+    run consecutive batches at the same time, so each batch must keep its own image-summed
+    targets (the two halves of the replay buffer) until the batch after next."""
+    import ctypes
+    from libgint_b200.capi import load_engine
+    lib = load_engine()
+    wl = Workload("periodic_l2_small")
+    s = Session(Api(engine_so), wl, max_mem_mb=150)
+    h = ctypes.c_void_p(s.h)
+    lib.libgint_record(h, 1)
+    K1, _, _ = s.build_K()
+    lib.libgint_record(h, 0)
+    stats = (ctypes.c_longlong * 8)()
+    lib.libgint_get_stats(h, stats)
+    assert stats[3] >= 4, f"expected a recording of several batches, got {stats[3]}"
+    P = wl.Pflat
+    lib.libgint_set_P(h, P.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), P.size)
+    K2 = np.zeros_like(K1)
+    for _ in range(2):
+        assert lib.libgint_replay(h) > 0 and lib.libgint_last_error(h) == 0
+        lib.libgint_get_K(h, K2.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        assert np.abs(K1 - K2).max() <= 1e-13 * np.abs(K1).max()
+    s.close()
+
+
+@pytest.mark.gpu
 def test_out_of_range_update_is_an_error(engine_so):
     """An add_qrtt offset beyond P_size is caught by the kernel's bounds check (no fault)."""
     from libgint_b200.capi import LibGint
