@@ -234,6 +234,7 @@ def run_ours(args, world, rank, local):
     err = lib.libgint_last_error(h)
     if err:
         raise RuntimeError(f"engine error {err}: {lib.libgint_error_string(h).decode()}")
+    K0_local = K0.copy()
     K0 = sum_K(K0)
 
     # 2) value: device-resident K builds (replay), timed with CUDA events on the engine stream
@@ -250,6 +251,14 @@ def run_ours(args, world, rank, local):
     barrier()
     clk = clocks.stop()
     check()
+    # the replayed K (same P as the recorded build) must be the streamed build's K; checked after
+    # the timed region, so the timed replays are the ones whose result is verified
+    Krep = np.zeros_like(K0_local)
+    lib.libgint_get_K(h, Krep.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    check()
+    replay_dev = max_over_ranks(float(np.abs(Krep - K0_local).max() / max(1e-300, np.abs(K0_local).max())))
+    if not replay_dev <= 1e-12:
+        raise RuntimeError(f"replayed K differs from the streamed build's K: rel max|dK| = {replay_dev:.3e}")
     lib.libgint_get_stats(h, stats)
     launches = (stats[4] - launches0) // max(1, args.steps)
     tot_ms = max_over_ranks(float(np.sum(step_ms)))
@@ -289,6 +298,7 @@ def run_ours(args, world, rank, local):
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "ms_per_step": ms_per_step,
                               "device_only": True, "k_builds": args.warmup + args.steps + 2,
+                              "replay_rel_max_dK_vs_stream": replay_dev,
                               "kernel_ms_per_step": kt[0], "group_kernel_ms_per_step": kt[1]}), flush=True)
         if pg:
             torch.distributed.destroy_process_group()
@@ -391,6 +401,7 @@ def run_ours(args, world, rank, local):
                          "kernel_ms_per_step": kt[0], "group_kernel_ms_per_step": kt[1],
                          "flops_per_step": flops_prim, "images_evaluated": int(n_img)},
             "clocks": clk,
+            "replay_rel_max_dK_vs_stream": replay_dev,
         }
         if cpu:
             line["cpu_baseline"] = cpu
