@@ -796,14 +796,16 @@ cudaError_t upload_constant_tables(const double *c2s_l0to3, const double *symm5)
 
 int plan_smem_doubles() { return (int)((sizeof(ClassPlan) + 15) / 16) * 2; }
 
-static int g_max_smem = 0;
+// the opt-in shared memory per block of the first device asked (the engine's GPUs are all one
+// type); a function-local static, so concurrent caller threads initialise it once
 static int max_dyn_smem() {
-   if (!g_max_smem) {
-      int dev = 0; cudaGetDevice(&dev);
-      cudaDeviceGetAttribute(&g_max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-      if (g_max_smem <= 0) g_max_smem = 48 * 1024;
-   }
-   return g_max_smem;
+   static const int smax = [] {
+      int dev = 0, v = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+      return v > 0 ? v : 48 * 1024;
+   }();
+   return smax;
 }
 
 template <int TS>
@@ -843,22 +845,21 @@ static void prim2_shape(const ClassPlan &hp, bool lane_vrr, int *cp, size_t *war
 
 static bool prim2_lane(const ClassPlan &hp) { return hp.V <= 96; }
 
-static int g_prim_kernel = -1;
 
 // Primitive-kernel choice: k_prim3 (generated VRR) for the classes it covers, then k_prim2,
 // then the team kernel for the largest classes. LIBGINT_PRIM_KERNEL=2 skips k_prim3 and =1 uses
 // the team kernel only (for comparisons).
 cudaError_t launch_prim(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan &hp, cudaStream_t st) {
    if (bt.nprm == 0) return cudaSuccess;
-   if (g_prim_kernel < 0) {
+   static const int prim_kernel = [] {
       const char *e = getenv("LIBGINT_PRIM_KERNEL");
-      g_prim_kernel = (e && e[0] == '1') ? 1 : ((e && e[0] == '2') ? 2 : 3);
-   }
-   if (g_prim_kernel == 3) {
+      return (e && e[0] == '1') ? 1 : ((e && e[0] == '2') ? 2 : 3);
+   }();
+   if (prim_kernel == 3) {
       cudaError_t err = cudaSuccess;
       if (prim3_launch(ctx, bt, st, &err)) return err;
    }
-   if (g_prim_kernel >= 2) {
+   if (prim_kernel >= 2) {
       const bool lane = prim2_lane(hp);
       int cp = 1;
       size_t wd = 0;
@@ -911,17 +912,16 @@ size_t group_global_scratch(const ClassPlan &hp, int *grid, int *warps) {
    return wd * (size_t)(*warps) * (*grid);
 }
 
-static int g_group_kernel = -1;
 
 // Group-kernel choice: k_group3 (generated HRR, one lane per group) for the classes it covers,
 // then k_group_lane / k_group. LIBGINT_GROUP_KERNEL=2 skips k_group3 (for comparisons).
 cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan &hp, cudaStream_t st) {
    if (bt.ngroup == 0) return cudaSuccess;
-   if (g_group_kernel < 0) {
+   static const int group_kernel = [] {
       const char *e = getenv("LIBGINT_GROUP_KERNEL");
-      g_group_kernel = (e && e[0] == '2') ? 2 : 3;
-   }
-   if (g_group_kernel == 3) {
+      return (e && e[0] == '2') ? 2 : 3;
+   }();
+   if (group_kernel == 3) {
       cudaError_t err = cudaSuccess;
       if (group3_launch(ctx, bt, st, &err)) return err;
    }
