@@ -111,6 +111,12 @@ void libgint_destroy_handle(void *handle);
  * targets, HRR workspace (doubles), cartesian and spherical block sizes, VRR blocks, HRR
  * steps, primitive team size; returns 0 for an unsupported class */
 int libgint_plan_sizes(int la, int lb, int lc, int ld, int *out);
+/* the HRR instructions of class (la,lb,lc,ld) as the interpreted group kernel runs them: out[2i],
+ * out[2i+1] = {in1 | axis << 30, in2} computing workspace element S + i as
+ * w[S+i] = w[in1] + R[axis] * w[in2] (R = C - D for the first info[3] elements, A - B after), up to
+ * cap instructions; info[0..3] = S, H, offset of the final cartesian block, ket elements. Returns the
+ * instruction count (-1: unsupported class). No GPU needed. */
+int libgint_hrr_program(int la, int lb, int lc, int ld, unsigned int *out, int cap, int *info);
 /* on = 1: keep the device batches of the following K build(s) (the screened quartet list of
  * an SCF step); on = 0: stop recording */
 void libgint_record(void *handle, int on);

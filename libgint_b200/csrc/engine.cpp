@@ -1359,6 +1359,30 @@ int libgint_plan_sizes(int la, int lb, int lc, int ld, int *out) {
    return 1;
 }
 
+// The HRR instructions the interpreted group kernel runs for one class (host copy of the per-GPU
+// table, build_group_prog): out[2i], out[2i+1] = {in1 | axis << 30, in2} of workspace element
+// S + i, up to cap instructions; info[0..3] = S, H, the offset of the final cartesian block, the
+// number of ket elements (the first ones; they use CD, the rest AB). Returns the number of
+// instructions, -1 for an unsupported class. Needs no GPU.
+int libgint_hrr_program(int la, int lb, int lc, int ld, unsigned int *out, int cap, int *info) {
+   ClassPlan p;
+   if (la < 0 || lb < 0 || lc < 0 || ld < 0 || la > kMaxL || lb > kMaxL || lc > kMaxL || ld > kMaxL ||
+       !build_class_plan(la, lb, lc, ld, p))
+      return -1;
+   static std::vector<uint2> prog;
+   static std::once_flag built;
+   std::call_once(built, [] { build_group_prog(prog); });
+   if (prog.empty()) return -1;
+   const int c = la * 64 + lb * 16 + lc * 4 + ld;
+   const uint32_t first = prog[c].x, end = c + 1 < 256 ? prog[c + 1].x : (uint32_t)prog.size();
+   const int n = (int)(end - first);
+   for (int i = 0; i < n && i < cap; i++) { out[2 * i] = prog[first + i].x; out[2 * i + 1] = prog[first + i].y; }
+   int ket = 0;
+   for (int o = 0; o < p.nhop; o++) if (p.hop[o].type == 0) ket += p.hop[o].nelem;
+   if (info) { info[0] = p.S; info[1] = p.H; info[2] = p.out_off; info[3] = ket; }
+   return n;
+}
+
 const char *libgint_error_string(void *hh) { return ((Handle *)hh)->errmsg.c_str(); }
 
 void libgint_destroy_handle(void *hh) {
