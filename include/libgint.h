@@ -117,6 +117,14 @@ int libgint_plan_sizes(int la, int lb, int lc, int ld, int *out);
  * cap instructions; info[0..3] = S, H, offset of the final cartesian block, ket elements. Returns the
  * instruction count (-1: unsupported class). No GPU needed. */
 int libgint_hrr_program(int la, int lb, int lc, int ld, unsigned int *out, int cap, int *info);
+/* the precompiled VRR instructions of class (la,lb,lc,ld) as the large-class primitive kernels run
+ * them, in order: 16-byte records {int16 out, i0..i4; uint8 zA, kind; int8 f1, f2}, up to cap;
+ *   kind 0: w[out] = z[zA] w[i0] + z[zA+3] w[i1] + f1 (z[12] w[i2] + z[13] w[i3])
+ *   kind 1: w[out] = z[zA] w[i0] + z[zA+3] w[i1] + f1 (z[14] w[i2] + z[15] w[i3]) + f2 z[16] w[i4]
+ * (terms with a zero multiplier are left out; absent inputs point at a zero at w[V]); info = V, S,
+ * (0|0)^(m) count at w[0..], ntg, then per target {workspace offset, target offset, length, e, f},
+ * info_cap >= 4 + 5 ntg. Returns the instruction count (-1: unsupported class). No GPU needed. */
+int libgint_vrr_program(int la, int lb, int lc, int ld, void *vops, int cap, int *info, int info_cap);
 /* on = 1: keep the device batches of the following K build(s) (the screened quartet list of
  * an SCF step); on = 0: stop recording */
 void libgint_record(void *handle, int on);

@@ -45,6 +45,7 @@ SIGNATURES = {
     "libgint_destroy_handle": (None, [_V]),
     "libgint_plan_sizes": (ctypes.c_int, [ctypes.c_int] * 4 + [_I]),
     "libgint_hrr_program": (ctypes.c_int, [ctypes.c_int] * 4 + [ctypes.POINTER(ctypes.c_uint), ctypes.c_int, _I]),
+    "libgint_vrr_program": (ctypes.c_int, [ctypes.c_int] * 4 + [_V, ctypes.c_int, _I, ctypes.c_int]),
     "libgint_record": (None, [_V, ctypes.c_int]),
     "libgint_replay": (ctypes.c_double, [_V]),
     "libgint_replay_profile": (ctypes.c_double, [_V, _D]),

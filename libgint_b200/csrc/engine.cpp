@@ -1383,6 +1383,29 @@ int libgint_hrr_program(int la, int lb, int lc, int ld, unsigned int *out, int c
    return n;
 }
 
+// The precompiled VRR instructions of one class (build_vops), as k_prim2 and k_prim run them
+// level after level: 16-byte VOp records (engine_types.h) into vops, up to cap of them. info gets
+// V, S, the number of (0|0)^(m) values at the start of the workspace, the number of targets ntg,
+// then per target its workspace offset, target offset, length and (e, f) shells; info_cap >= 4 +
+// 5 ntg. Returns the instruction count, -1 for an unsupported class. Needs no GPU.
+int libgint_vrr_program(int la, int lb, int lc, int ld, void *vops, int cap, int *info, int info_cap) {
+   ClassPlan p;
+   if (la < 0 || lb < 0 || lc < 0 || ld < 0 || la > kMaxL || lb > kMaxL || lc > kMaxL || ld > kMaxL ||
+       !build_class_plan(la, lb, lc, ld, p))
+      return -1;
+   std::vector<VOp> v;
+   build_vops(p, v);
+   if (vops) std::memcpy(vops, v.data(), sizeof(VOp) * std::min<size_t>(v.size(), (size_t)std::max(cap, 0)));
+   if (info && info_cap >= 4 + 5 * p.ntg) {
+      info[0] = p.V; info[1] = p.S; info[2] = p.vb[0].nm; info[3] = p.ntg;
+      for (int t = 0; t < p.ntg; t++) {
+         int *q = info + 4 + 5 * t;
+         q[0] = p.tg_voff[t]; q[1] = p.tg_soff[t]; q[2] = p.tg_n[t]; q[3] = p.tg_e[t]; q[4] = p.tg_f[t];
+      }
+   }
+   return (int)v.size();
+}
+
 const char *libgint_error_string(void *hh) { return ((Handle *)hh)->errmsg.c_str(); }
 
 void libgint_destroy_handle(void *hh) {

@@ -127,3 +127,52 @@ def test_generated_vrr_matches_recursion(harness):
         mask = ~np.isnan(ref)
         assert np.array_equal(np.isnan(got), ~mask), c
         assert np.array_equal(got[mask], ref[mask]), (c, np.abs(got[mask] - ref[mask]).max())
+
+
+_VOP = np.dtype([("out", "<i2"), ("i0", "<i2"), ("i1", "<i2"), ("i2", "<i2"), ("i3", "<i2"), ("i4", "<i2"),
+                 ("zA", "u1"), ("kind", "u1"), ("f1", "i1"), ("f2", "i1")])
+
+
+def _run_vops(lib, la, lb, lc, ld, F, z):
+    """Runs the engine's precompiled VRR instructions of one class (libgint_vrr_program) in order,
+    with the formula the large-class primitive kernels apply, and gathers the targets."""
+    info = (ctypes.c_int * (4 + 5 * 64))()
+    n = lib.libgint_vrr_program(la, lb, lc, ld, None, 0, info, len(info))
+    buf = np.zeros(max(n, 1), dtype=_VOP)
+    assert lib.libgint_vrr_program(la, lb, lc, ld, buf.ctypes.data, n, info, len(info)) == n
+    V, S, n00, ntg = info[0], info[1], info[2], info[3]
+    w = [0.0] * (V + 1)
+    for q in range(n00):
+        w[q] = F[q]
+    for o in buf[:n].tolist():
+        out, i0, i1, i2, i3, i4, zA, kind, f1, f2 = o
+        v = z[zA] * w[i0] + z[zA + 3] * w[i1]
+        if f1:
+            v += f1 * (z[12 + 2 * kind] * w[i2] + z[13 + 2 * kind] * w[i3])
+        if f2:
+            v += f2 * z[16] * w[i4]
+        w[out] = v
+    got = np.full(S, np.nan)
+    for t in range(ntg):
+        voff, soff, cnt, e, f = info[4 + 5 * t:9 + 5 * t]
+        if la == 0 and lc == 0 and e == 0 and f == 0:
+            continue          # the (00|00) target is summed over every image by the kernels
+        got[soff:soff + cnt] = w[voff:voff + cnt]
+    return got
+
+
+@pytest.mark.parametrize("c", range(256), ids=lambda c: "%d%d%d%d" % (c >> 6, (c >> 4) & 3, (c >> 2) & 3, c & 3))
+def test_vrr_instructions_match_recursion(c):
+    """The VRR instruction table of every class (k_prim2 and the team kernel run it on the GPU)
+    gives the recursion's targets bit for bit: same operations in the same order."""
+    from libgint_b200.capi import load_engine
+    lib = load_engine()
+    la, lb, lc, ld = c >> 6, (c >> 4) & 3, (c >> 2) & 3, c & 3
+    rng = np.random.default_rng(1000 + c)
+    F = tuple(rng.uniform(0.1, 1.0, la + lb + lc + ld + 1).tolist())
+    z = tuple(rng.uniform(-1.0, 1.0, 17).tolist())
+    ref = _reference(la, lb, lc, ld, F, z)
+    got = _run_vops(lib, la, lb, lc, ld, F, z)
+    mask = ~np.isnan(ref)
+    assert np.array_equal(np.isnan(got), ~mask), c
+    assert np.array_equal(got[mask], ref[mask]), (c, np.abs(got[mask] - ref[mask]).max())
