@@ -17,7 +17,8 @@ HOSTCXX = "g++"
 # generated classes compile in parallel
 PRIM3_PARTS = 8
 GROUP3_PARTS = 4
-ENGINE_OBJS = [("engine.cpp", [], "engine.o"), ("plan.cpp", [], "plan.o"), ("kernels.cu", [], "kernels.o")] + \
+# engine.cpp holds the team-collective calls (orphaned OpenMP constructs bound to the caller's team)
+ENGINE_OBJS = [("engine.cpp", ["-Xcompiler", "-fopenmp"], "engine.o"), ("plan.cpp", [], "plan.o"), ("kernels.cu", [], "kernels.o")] + \
     [("prim3.cu", [f"-DPRIM3_PART={i}"], f"prim3_{i}.o") for i in range(PRIM3_PARTS)] + \
     [("group3.cu", [f"-DGROUP3_PART={i}"], f"group3_{i}.o") for i in range(GROUP3_PARTS)]
 DRIVER_SRC = ["driver.cpp"]
@@ -63,7 +64,7 @@ def build_engine(force=False, verbose=False):
     objs = [os.path.join(OBJDIR, o) for _, _, o in ENGINE_OBJS]
     if force or jobs or _stale(out, objs):
         os.makedirs(LIB, exist_ok=True)
-        logs.append(_run([NVCC] + ARCH + ["-shared", "-o", out] + objs + ["-lcudart"]))
+        logs.append(_run([NVCC] + ARCH + ["-shared", "-o", out] + objs + ["-lcudart", "-lgomp"]))
     if verbose:
         print("\n".join(logs))
     return out
@@ -74,7 +75,7 @@ def build_driver(force=False):
     srcs = [os.path.join(CSRC, f) for f in DRIVER_SRC]
     if force or _stale(out, srcs):
         os.makedirs(LIB, exist_ok=True)
-        _run([HOSTCXX, "-O2", "-std=c++17", "-fPIC", "-shared", "-o", out] + srcs + ["-ldl"])
+        _run([HOSTCXX, "-O2", "-std=c++17", "-fPIC", "-fopenmp", "-shared", "-o", out] + srcs + ["-ldl"])
     return out
 
 

@@ -17,6 +17,8 @@
 // each patch (patch geometry in tcg_patches.h).
 #include <algorithm>
 #include <array>
+#include <atomic>
+#include <functional>
 #include <chrono>
 #include <cmath>
 #include <cstdint>
@@ -24,6 +26,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <dlfcn.h>
+#include <omp.h>
 #include <string>
 #include <thread>
 #include <vector>
@@ -186,6 +189,9 @@ struct gd_config {
    int full_enum;       // 1: all (i,j,k,l) with factor 0.25 instead of the unique quartets
    int max_prm;         // max primitives per set for the l<=3 basis (<=16)
    int max_ncontr;      // max contractions per set for the l<=3 basis (<=4)
+   int setq_stride;     // > 1: keep the candidate set quartets (i,j,k,l) whose hash is setq_phase
+   int setq_phase;      //      modulo setq_stride (a uniform sample of a workload too large to run whole)
+   int threads;         // enumeration threads (0: all hardware threads); the result does not depend on it
 };
 
 struct gd_info {
@@ -485,73 +491,129 @@ gd_workload *gd_create(const gd_config *cfg) {
       pr.rad = 0.5 * std::sqrt(AB2) + (zmin < 1e299 ? std::sqrt(27.6 / zmin) : 0.0);
    };
    std::vector<std::vector<Pair>> pairs((size_t)S * S);
-   for (int a = 0; a < S; a++) for (int b = 0; b < S; b++) {
-      if (!cfg->full_enum && b > a) continue;
-      for (int n1 = 0; n1 < w->Ng; n1++) {
-         Pair pr; pair_of(a, b, n1, pr);
-         if (pr.Q * 10.0 < eps) continue;   // negligible pair even against |P| ~ 10
-         pairs[(size_t)a * S + b].push_back(std::move(pr));
+   const int nth = cfg->threads > 0 ? cfg->threads : std::max(1, (int)std::thread::hardware_concurrency());
+   // rows a of the pair table (and below, the first set i of the quartets) are handed out to the
+   // threads one at a time; every row is written by one thread, so the result is the serial one
+   auto parallel_rows = [&](const std::function<void(int)> &fn) {
+      std::atomic<int> next{0};
+      std::vector<std::thread> th;
+      for (int t = 0; t < nth; t++)
+         th.emplace_back([&]() { for (int r; (r = next.fetch_add(1)) < S;) fn(r); });
+      for (auto &x : th) x.join();
+   };
+   parallel_rows([&](int a) {
+      for (int b = 0; b < S; b++) {
+         if (!cfg->full_enum && b > a) continue;
+         for (int n1 = 0; n1 < w->Ng; n1++) {
+            Pair pr; pair_of(a, b, n1, pr);
+            if (pr.Q * 10.0 < eps) continue;   // negligible pair even against |P| ~ 10
+            pairs[(size_t)a * S + b].push_back(std::move(pr));
+         }
       }
-   }
-   // ---- quartet enumeration
+   });
+   // ---- quartet enumeration: each first set i is enumerated by one thread into its own lists,
+   // which are then joined in the order of i
    auto pidx = [&](int a, int b) { return (long)a * S + b; };
    const double rc = w->rc_bohr;
-   for (int i = 0; i < S; i++) for (int j = 0; j < S; j++) {
+   struct Part { std::vector<SetQ> setq; std::vector<Shell> shells; std::vector<uint32_t> prims; long n_qrtt = 0; };
+   std::vector<Part> parts(S);
+   const uint64_t stride = cfg->setq_stride > 1 ? (uint64_t)cfg->setq_stride : 1;
+   const uint64_t phase = cfg->setq_stride > 1 ? (uint64_t)cfg->setq_phase % stride : 0;
+   // Set quartets in canonical order: (i,j) >= (k,l) with i >= j, k >= l. With setq_stride > 1 only
+   // every stride-th ket pair index of each row is visited, from an offset that a hash of the bra
+   // pair picks (a sample of 1/stride of the set quartets whose cost does not grow with the
+   // workload's full size).
+   parallel_rows([&](int i) {
+   Part &out = parts[i];
+   auto visit = [&](int j, int k, int l, const std::vector<Pair> &PL) {
+      const auto &QL = pairs[(size_t)pidx(k, l)];
+      if (QL.empty()) return;
+      double pmax = std::max(std::max(Pblk[(size_t)i * S + k], Pblk[(size_t)i * S + l]),
+                             std::max(Pblk[(size_t)j * S + k], Pblk[(size_t)j * S + l]));
+      const SetDef &da = w->defs[w->sets[i].def], &db = w->defs[w->sets[j].def];
+      const SetDef &dc = w->defs[w->sets[k].def], &dd = w->defs[w->sets[l].def];
+      SetQ sq; sq.i = i; sq.j = j; sq.k = k; sq.l = l;
+      if (cfg->full_enum) sq.fac = 0.25f;
+      else {
+         double f = 2.0;
+         if (i == j) f *= 0.5;
+         if (k == l) f *= 0.5;
+         if (i == k && j == l) f *= 0.5;
+         sq.fac = (float)f;
+      }
+      sq.shell_begin = (uint32_t)out.shells.size();
+      for (const Pair &pa : PL) for (const Pair &pc : QL) {
+         if (pa.Q * pc.Q * pmax < eps) continue;
+         // truncated-Coulomb range: the nearest image of the ket distribution must be in reach
+         double d2 = 0;
+         for (int q = 0; q < 3; q++) {
+            double d = pa.ctr[q] - pc.ctr[q];
+            if (periodic) d -= Lb * std::round(d / Lb);
+            d2 += d * d;
+         }
+         double lim = rc + pa.rad + pc.rad;
+         bool reach = d2 <= lim * lim;
+         if (!reach) continue;
+         Shell sh; sh.n1 = (uint16_t)pa.n1; sh.n2 = (uint16_t)pc.n1;
+         sh.prm_begin = (uint32_t)out.prims.size();
+         for (int ia = 0; ia < da.np; ia++) for (int ib = 0; ib < db.np; ib++) {
+            double qab = pa.q[(size_t)ia * db.np + ib];
+            if (qab * pc.Q * pmax < eps) continue;
+            for (int ic = 0; ic < dc.np; ic++) for (int id = 0; id < dd.np; id++) {
+               double qcd = pc.q[(size_t)ic * dd.np + id];
+               if (qab * qcd * pmax < eps) continue;
+               out.prims.push_back(((uint32_t)ia << 24) | ((uint32_t)ib << 16) | ((uint32_t)ic << 8) | (uint32_t)id);
+            }
+         }
+         sh.prm_end = (uint32_t)out.prims.size();
+         if (sh.prm_end > sh.prm_begin) out.shells.push_back(sh);
+      }
+      sq.shell_end = (uint32_t)out.shells.size();
+      if (sq.shell_end > sq.shell_begin) {
+         out.setq.push_back(sq);
+         out.n_qrtt += (long)da.nl * db.nl * dc.nl * dd.nl;
+      }
+   };
+   for (int j = 0; j < S; j++) {
       if (!cfg->full_enum && j > i) continue;
       const auto &PL = pairs[(size_t)pidx(i, j)];
       if (PL.empty()) continue;
-      for (int k = 0; k < S; k++) for (int l = 0; l < S; l++) {
-         if (!cfg->full_enum) {
-            if (l > k) continue;
-            if (k > i || (k == i && l > j)) continue;   // canonical: (i,j) >= (k,l)
-         }
-         const auto &QL = pairs[(size_t)pidx(k, l)];
-         if (QL.empty()) continue;
-         double pmax = std::max(std::max(Pblk[(size_t)i * S + k], Pblk[(size_t)i * S + l]),
-                                std::max(Pblk[(size_t)j * S + k], Pblk[(size_t)j * S + l]));
-         const SetDef &da = w->defs[w->sets[i].def], &db = w->defs[w->sets[j].def];
-         const SetDef &dc = w->defs[w->sets[k].def], &dd = w->defs[w->sets[l].def];
-         SetQ sq; sq.i = i; sq.j = j; sq.k = k; sq.l = l;
-         if (cfg->full_enum) sq.fac = 0.25f;
-         else {
-            double f = 2.0;
-            if (i == j) f *= 0.5;
-            if (k == l) f *= 0.5;
-            if (i == k && j == l) f *= 0.5;
-            sq.fac = (float)f;
-         }
-         sq.shell_begin = (uint32_t)w->shells.size();
-         for (const Pair &pa : PL) for (const Pair &pc : QL) {
-            if (pa.Q * pc.Q * pmax < eps) continue;
-            // truncated-Coulomb range: the nearest image of the ket distribution must be in reach
-            double d2 = 0;
-            for (int q = 0; q < 3; q++) {
-               double d = pa.ctr[q] - pc.ctr[q];
-               if (periodic) d -= Lb * std::round(d / Lb);
-               d2 += d * d;
-            }
-            double lim = rc + pa.rad + pc.rad;
-            bool reach = d2 <= lim * lim;
-            if (!reach) continue;
-            Shell sh; sh.n1 = (uint16_t)pa.n1; sh.n2 = (uint16_t)pc.n1;
-            sh.prm_begin = (uint32_t)w->prims.size();
-            for (int ia = 0; ia < da.np; ia++) for (int ib = 0; ib < db.np; ib++) {
-               double qab = pa.q[(size_t)ia * db.np + ib];
-               if (qab * pc.Q * pmax < eps) continue;
-               for (int ic = 0; ic < dc.np; ic++) for (int id = 0; id < dd.np; id++) {
-                  double qcd = pc.q[(size_t)ic * dd.np + id];
-                  if (qab * qcd * pmax < eps) continue;
-                  w->prims.push_back(((uint32_t)ia << 24) | ((uint32_t)ib << 16) | ((uint32_t)ic << 8) | (uint32_t)id);
-               }
-            }
-            sh.prm_end = (uint32_t)w->prims.size();
-            if (sh.prm_end > sh.prm_begin) w->shells.push_back(sh);
-         }
-         sq.shell_end = (uint32_t)w->shells.size();
-         if (sq.shell_end > sq.shell_begin) {
-            w->setq.push_back(sq);
-            w->n_qrtt += (long)da.nl * db.nl * dc.nl * dd.nl;
-         }
+      if (cfg->full_enum) {
+         for (int k = 0; k < S; k++) for (int l = 0; l < S; l++) visit(j, k, l, PL);
+         continue;
+      }
+      const uint64_t pij = (uint64_t)i * (i + 1) / 2 + j;   // ket pairs (k,l) <= (i,j): indices 0..pij
+      uint64_t kl = 0;
+      if (stride > 1) {
+         uint64_t x = pij + 0x9e3779b97f4a7c15ULL;   // splitmix64 of the bra pair index
+         x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ULL;
+         x = (x ^ (x >> 27)) * 0x94d049bb133111ebULL;
+         x ^= x >> 31;
+         kl = (x + phase) % stride;
+      }
+      int k = 0;
+      for (; kl <= pij; kl += stride) {
+         while ((uint64_t)(k + 1) * (k + 2) / 2 <= kl) k++;
+         visit(j, k, (int)(kl - (uint64_t)k * (k + 1) / 2), PL);
+      }
+   }
+   });
+   {
+      size_t nsq = 0, nsh = 0, npr = 0;
+      for (const Part &pt : parts) { nsq += pt.setq.size(); nsh += pt.shells.size(); npr += pt.prims.size(); }
+      if (npr > 0xffffffffull || nsh > 0xffffffffull) {
+         fprintf(stderr, "gd_create: %zu primitive quartets exceed the 32-bit trace indices; use setq_stride\n", npr);
+         delete w;
+         return nullptr;
+      }
+      w->setq.reserve(nsq); w->shells.reserve(nsh); w->prims.reserve(npr);
+      for (Part &pt : parts) {
+         const uint32_t sh0 = (uint32_t)w->shells.size(), pr0 = (uint32_t)w->prims.size();
+         for (SetQ q : pt.setq) { q.shell_begin += sh0; q.shell_end += sh0; w->setq.push_back(q); }
+         for (Shell h : pt.shells) { h.prm_begin += pr0; h.prm_end += pr0; w->shells.push_back(h); }
+         w->prims.insert(w->prims.end(), pt.prims.begin(), pt.prims.end());
+         w->n_qrtt += pt.n_qrtt;
+         std::vector<SetQ>().swap(pt.setq); std::vector<Shell>().swap(pt.shells); std::vector<uint32_t>().swap(pt.prims);
       }
    }
    // ---- C0
@@ -623,6 +685,15 @@ long gd_get_shells(const gd_workload *w, long q, long *out) {
       out[n * 3 + 2] = w->shells[h].prm_end - w->shells[h].prm_begin;
    }
    return n;
+}
+
+// primitive-quartet codes (ipa<<24 | ipb<<16 | ipc<<8 | ipd) of shell quartet h (index in the
+// workload's shell list, set quartet q's shells are [sum of earlier n_shells, + n_shells)); returns
+// the count
+long gd_get_shell_prims(const gd_workload *w, long h, uint32_t *out) {
+   const Shell &sh = w->shells[h];
+   std::memcpy(out, &w->prims[sh.prm_begin], sizeof(uint32_t) * (sh.prm_end - sh.prm_begin));
+   return (long)(sh.prm_end - sh.prm_begin);
 }
 
 // per set quartet {i,j,k,l,n_shells,n_prims} (for cost/class statistics)
@@ -917,6 +988,37 @@ double gd_build_K_mt(const gd_workload *w, gd_api *a, void **handles, int nh, co
       times[4] = ms(t1, t2);
    }
    return ms(t0, t2);
+}
+
+// One K build by an OpenMP team of nh threads, as CP2K's HFX module drives the libGint C-ABI from
+// its OpenMP team: thread t uses handles[t] and streams the set quartets [cut[t], cut[t+1])
+// (positions in idx[] when idx is given), and every thread passes the same P and K arrays. The
+// library's set_P and get_K are collective over the team, so K receives the team's whole K with
+// no summation by the caller. Returns wall ms (-1 if the team did not get nh threads); times as
+// gd_build_K_mt, with times[4] = 0.
+double gd_build_K_team(const gd_workload *w, gd_api *a, void **handles, int nh, const double *P, double *K,
+                       const long *idx, const long *cut, double *times) {
+   using clk = std::chrono::steady_clock;
+   std::vector<double> tt(3 * nh, 0.0), tw(nh, 0.0);
+   int got = 0;
+   auto t0 = clk::now();
+   omp_set_dynamic(0);
+#pragma omp parallel num_threads(nh)
+   {
+      const int t = omp_get_thread_num();
+#pragma omp single
+      got = omp_get_num_threads();
+      if (got == nh)
+         tw[t] = build_K_impl(w, a, handles[t], P, K, cut[t], cut[t + 1], idx, &tt[3 * t], g_bulk != 0);
+   }
+   auto t1 = clk::now();
+   if (got != nh) return -1.0;
+   if (times) {
+      for (int i = 0; i < 3; i++) times[i] = tt[i];
+      times[3] = *std::max_element(tw.begin(), tw.end());
+      times[4] = 0.0;
+   }
+   return std::chrono::duration<double, std::milli>(t1 - t0).count();
 }
 
 void gd_teardown(gd_api *a, void *h) { if (a->destroy) a->destroy(h); }

@@ -12,11 +12,15 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
 
 #include <cuda_runtime.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 #include "../../include/libgint.h"
 #include "engine_types.h"
@@ -202,12 +206,31 @@ struct ClassQ {
    PVec<ShellRec> shells;
    PVec<GroupRec> groups;
    PVec<QrttRec> qrtts;
+   PVec<uint32_t> rowgrp;           // group of contraction row 32 k (filled when the batch is packed)
    bool active = false;
 };
 
 struct DBuf {
    void *p = nullptr;
    size_t bytes = 0;
+};
+
+// The device P and K of a K build. As in the reference (src/libGint.cpp:436-447, 555-562,
+// 613-628), the handles of one OpenMP team share them: libgint_set_P, libgint_set_K and
+// libgint_get_K are collective over the calling thread's team (orphaned omp constructs bind to
+// it), one thread uploads P and zeroes K for all, every handle's kernels add into the one K, and
+// get_K copies the team's K once after a barrier. A handle used outside a parallel region is a
+// team of one.
+struct Team {
+   int device = 0;
+   DBuf P[2], K[2];
+   int nspin = 0;
+   size_t FP_size = 0;
+   bool ok = false;     // P uploaded and K zeroed without an error
+   Team() = default;
+   Team(const Team &) = delete;
+   Team &operator=(const Team &) = delete;
+   ~Team();
 };
 
 struct Slot {
@@ -231,6 +254,7 @@ struct Handle {
    cudaEvent_t work_ev[kWorkStreams] = {};
    cudaEvent_t fork_ev = nullptr;
    cudaEvent_t batch_ev[2][kWorkStreams] = {};   // replay: each worker's end of the last batch of each parity
+   cudaEvent_t noalloc_ev = nullptr;             // libgint_replay_noalloc: the caller's stream waits for the handle's
    int err = 0;
    std::string errmsg;
    // potential and tables
@@ -254,7 +278,7 @@ struct Handle {
    // device-resident data
    DBuf d_pool, d_ents, d_neighs, d_C0, d_lut, d_bw, d_ft, d_plans, d_err, d_vops;
    std::vector<VOp> vops;           // precompiled VRR instructions of all classes
-   DBuf d_P[2], d_K[2];
+   std::shared_ptr<Team> team;      // device P and K (shared by the handles of an OpenMP team)
    int nspin = 0;
    size_t FP_size = 0;
    ClassPlan plans[256];
@@ -272,7 +296,7 @@ struct Handle {
    Slot slots[2];
    int cur = 0;
    // record / replay of the device-resident quartet list
-   struct RecSeg { int c; size_t o_prm, o_ps, o_sh, o_g, o_q, ac_off; uint32_t nprm, nshell, ngroup; };
+   struct RecSeg { int c; size_t o_prm, o_ps, o_sh, o_g, o_q, o_rg, ac_off; uint32_t nprm, nshell, ngroup, nqrtt; };
    struct RecBatch { DBuf rec; std::vector<RecSeg> segs; size_t ac_doubles = 0; };
    bool recording = false;
    std::vector<RecBatch> recs;
@@ -305,6 +329,23 @@ static bool ensure(Handle *h, DBuf &b, size_t bytes, const char *what) {
 }
 
 static void release(DBuf &b) { if (b.p) cudaFree(b.p); b.p = nullptr; b.bytes = 0; }
+
+Team::~Team() {
+   int d = -1;
+   cudaGetDevice(&d);
+   if (d != device) cudaSetDevice(device);
+   for (int s = 0; s < 2; s++) { release(P[s]); release(K[s]); }
+   if (d >= 0 && d != device) cudaSetDevice(d);
+}
+
+// whether the calling thread is inside an OpenMP parallel region (a team of more than one)
+static bool in_team() {
+#ifdef _OPENMP
+   return omp_in_parallel() && omp_get_num_threads() > 1;
+#else
+   return false;
+#endif
+}
 
 static inline int cls_of(int la, int lb, int lc, int ld) { return la * 64 + lb * 16 + lc * 4 + ld; }
 
@@ -469,7 +510,10 @@ static DevCtx make_ctx(Handle *h) {
    c.lut_high = (const uint8_t *)h->d_lut.p + 128 * 128;
    c.bw = (const double *)h->d_bw.p;
    c.ftable = (const double *)h->d_ft.p;
-   for (int s = 0; s < 2; s++) { c.P[s] = (const double *)h->d_P[s].p; c.K[s] = (double *)h->d_K[s].p; }
+   for (int s = 0; s < 2; s++) {
+      c.P[s] = h->team ? (const double *)h->team->P[s].p : nullptr;
+      c.K[s] = h->team ? (double *)h->team->K[s].p : nullptr;
+   }
    c.hf_fac = h->hf_fac;
    c.FP_size = h->FP_size;
    c.err = (int *)h->d_err.p;
@@ -489,7 +533,7 @@ static inline size_t al16(size_t x) { return (x + 15) & ~(size_t)15; }
 static void clear_queues(Handle *h) {
    for (int c : h->active) {
       ClassQ &Q = h->q[c];
-      Q.prm.clear(); Q.prm_shell.clear(); Q.shells.clear(); Q.groups.clear(); Q.qrtts.clear();
+      Q.prm.clear(); Q.prm_shell.clear(); Q.shells.clear(); Q.groups.clear(); Q.qrtts.clear(); Q.rowgrp.clear();
       Q.active = false;
    }
    h->active.clear();
@@ -501,7 +545,7 @@ static void flush(Handle *h) {
    use_device(h);
    if (h->err) { clear_queues(h); return; }   // drop queued work after an error
    if (!upload_tables(h)) { clear_queues(h); return; }
-   if (h->nspin == 0 || !h->d_K[0].p) { set_error(h, 4, "work queued before libgint_set_P"); clear_queues(h); return; }
+   if (h->nspin == 0 || !h->team || !h->team->K[0].p) { set_error(h, 4, "work queued before libgint_set_P"); clear_queues(h); return; }
    if (!h->have_pot) { set_error(h, 4, "work queued before libgint_set_Potential_Truncated"); clear_queues(h); return; }
    for (int c : h->active) {
       if (h->ld_C0 < (h->plans[c].L + 1) * 105) {
@@ -512,12 +556,25 @@ static void flush(Handle *h) {
    }
    Slot &s = h->slots[h->cur];
    if (s.busy) { ck(h, cudaEventSynchronize(s.ev), "slot wait"); s.busy = false; }
-   // device layout of the batch: per class, prm | prm_shell | shells | groups | qrtts
-   struct Seg { int c; size_t o_prm, o_ps, o_sh, o_g, o_q; size_t ac_off; };
+   // device layout of the batch: per class, prm | prm_shell | shells | groups | qrtts | rowgrp
+   struct Seg { int c; size_t o_prm, o_ps, o_sh, o_g, o_q, o_rg; size_t ac_off; };
    std::vector<Seg> segs;
    size_t off = 0, ac = 0;
    for (int c : h->active) {
       ClassQ &Q = h->q[c];
+      // the group of every 32nd contraction row (rows are stored in group order)
+      const size_t nq = Q.qrtts.size(), nblk = (nq + 31) / 32;
+      Q.rowgrp.resize(nblk);
+      {
+         const GroupRec *gr = Q.groups.data();
+         const size_t ng = Q.groups.size();
+         size_t gi = 0;
+         for (size_t k = 0; k < nblk; k++) {
+            const size_t row = 32 * k;
+            while (gi + 1 < ng && gr[gi + 1].qrtt_off <= row) gi++;
+            Q.rowgrp.data()[k] = (uint32_t)gi;
+         }
+      }
       Seg g;
       g.c = c;
       g.o_prm = off; off = al16(off + Q.prm.size() * 4);
@@ -525,6 +582,7 @@ static void flush(Handle *h) {
       g.o_sh = off; off = al16(off + Q.shells.size() * sizeof(ShellRec));
       g.o_g = off; off = al16(off + Q.groups.size() * sizeof(GroupRec));
       g.o_q = off; off = al16(off + Q.qrtts.size() * sizeof(QrttRec));
+      g.o_rg = off; off = al16(off + Q.rowgrp.size() * 4);
       g.ac_off = ac;
       ac += ((size_t)Q.prm.size() * h->plans[c].S + 1) & ~(size_t)1;
       segs.push_back(g);
@@ -548,7 +606,8 @@ static void flush(Handle *h) {
       if (!up(g.o_prm, Q.prm.data(), Q.prm.size() * 4) || !up(g.o_ps, Q.prm_shell.data(), Q.prm_shell.size() * 4) ||
           !up(g.o_sh, Q.shells.data(), Q.shells.size() * sizeof(ShellRec)) ||
           !up(g.o_g, Q.groups.data(), Q.groups.size() * sizeof(GroupRec)) ||
-          !up(g.o_q, Q.qrtts.data(), Q.qrtts.size() * sizeof(QrttRec)))
+          !up(g.o_q, Q.qrtts.data(), Q.qrtts.size() * sizeof(QrttRec)) ||
+          !up(g.o_rg, Q.rowgrp.data(), Q.rowgrp.size() * 4))
          return;
    }
    h->h2d_bytes += (long long)off;
@@ -570,9 +629,11 @@ static void flush(Handle *h) {
       bt.shells = (const ShellRec *)(base + g.o_sh);
       bt.groups = (const GroupRec *)(base + g.o_g);
       bt.qrtts = (const QrttRec *)(base + g.o_q);
+      bt.rowgrp = (const uint32_t *)(base + g.o_rg);
       bt.nprm = (uint32_t)Q.prm.size();
       bt.nshell = (uint32_t)Q.shells.size();
       bt.ngroup = (uint32_t)Q.groups.size();
+      bt.nqrtt = (uint32_t)Q.qrtts.size();
       bt.AC = (double *)s.ac.p + g.ac_off;
       int gg = 0, gw = 0;
       size_t gs = group_global_scratch(hp, &gg, &gw);
@@ -584,7 +645,7 @@ static void flush(Handle *h) {
       if (!ck(h, launch_prim(ctx, bt, hp, ws), "k_prim launch")) return;
       if (!ck(h, launch_group(ctx, bt, hp, ws), "k_group launch")) return;
       h->n_launch += 2;
-      if (rb) rb->segs.push_back({g.c, g.o_prm, g.o_ps, g.o_sh, g.o_g, g.o_q, g.ac_off, bt.nprm, bt.nshell, bt.ngroup});
+      if (rb) rb->segs.push_back({g.c, g.o_prm, g.o_ps, g.o_sh, g.o_g, g.o_q, g.o_rg, g.ac_off, bt.nprm, bt.nshell, bt.ngroup, bt.nqrtt});
       h->n_prims += bt.nprm; h->n_shells += bt.nshell; h->n_groups += bt.ngroup;
    }
    join_workers(h);
@@ -601,7 +662,7 @@ static void flush(Handle *h) {
    for (int c = 0; c < 256; c++) {
       ClassQ &Q = h->q[c];
       if (Q.prm.size() || Q.shells.size() || Q.qrtts.size() || Q.groups.size()) {
-         Q.prm.clear(); Q.prm_shell.clear(); Q.shells.clear(); Q.groups.clear(); Q.qrtts.clear();
+         Q.prm.clear(); Q.prm_shell.clear(); Q.shells.clear(); Q.groups.clear(); Q.qrtts.clear(); Q.rowgrp.clear();
       }
       Q.active = false;
    }
@@ -617,34 +678,89 @@ static void drain(Handle *h) {
    }
 }
 
+// libgint_set_P: collective over the calling thread's OpenMP team (see Team). Every thread
+// reaches the same omp constructs whatever its own state, so that none waits at a barrier for
+// another that returned early.
 static void set_P_impl(Handle *h, int nspin, const double *Pa, const double *Pb, int n) {
    use_device(h);
-   if (n <= 0) { set_error(h, 2, "P_size must be positive"); return; }
-   // the previous build must be complete before P/K are replaced
+   const bool ok = n > 0;
+   if (!ok) set_error(h, 2, "P_size must be positive");
+   // this handle's previous build must be complete before P/K are replaced
    for (Slot &s : h->slots) if (s.busy) { ck(h, cudaEventSynchronize(s.ev), "slot wait"); s.busy = false; }
    ck(h, cudaStreamSynchronize(h->stream), "stream synchronize");
    for (Slot &s : h->slots) s.copy_busy = false;
-   h->nspin = nspin;
-   h->FP_size = (size_t)n;
-   const double *src[2] = {Pa, Pb};
-   for (int sp = 0; sp < nspin; sp++) {
-      if (!ensure(h, h->d_P[sp], (size_t)n * 8, "P") || !ensure(h, h->d_K[sp], (size_t)n * 8, "K")) return;
-      if (!h2d(h, h->d_P[sp].p, src[sp], (size_t)n * 8, "P upload")) return;
-      h->h2d_bytes += (long long)n * 8;
-      if (!ck(h, cudaMemsetAsync(h->d_K[sp].p, 0, (size_t)n * 8, h->stream), "K zero")) return;
+   std::shared_ptr<Team> *bc = nullptr;
+   const bool team_call = in_team();
+   // every handle of the team has finished its previous build
+#pragma omp barrier
+#pragma omp single copyprivate(bc)
+   {
+      // one thread uploads P and zeroes K for the team, reusing its team's buffers
+      std::shared_ptr<Team> t = (h->team && (team_call || h->team.use_count() == 1)) ? h->team : std::make_shared<Team>();
+      t->device = h->device;
+      t->nspin = nspin;
+      t->FP_size = ok ? (size_t)n : 0;
+      t->ok = false;
+      const double *src[2] = {Pa, Pb};
+      bool good = ok && !h->err;
+      for (int sp = 0; good && sp < nspin; sp++) {
+         good = ensure(h, t->P[sp], (size_t)n * 8, "P") && ensure(h, t->K[sp], (size_t)n * 8, "K") &&
+                h2d(h, t->P[sp].p, src[sp], (size_t)n * 8, "P upload") &&
+                ck(h, cudaMemsetAsync(t->K[sp].p, 0, (size_t)n * 8, h->stream), "K zero");
+         if (good) h->h2d_bytes += (long long)n * 8;
+      }
+      // P is copied at call time (the caller may reuse its array), and the other threads' kernels
+      // read it once they leave this construct
+      t->ok = good && ck(h, cudaStreamSynchronize(h->stream), "P upload");
+      bc = new std::shared_ptr<Team>(t);
    }
-   // P is copied at call time (the caller may reuse its array)
-   if (!ck(h, cudaStreamSynchronize(h->stream), "P upload")) return;
+   h->team = *bc;
+   // every thread holds the team before the broadcast copy is released
+#pragma omp barrier
+#pragma omp single nowait
+   delete bc;
+   h->nspin = nspin;
+   h->FP_size = h->team->FP_size;
+   if (!h->team->ok) set_error(h, 4, "libgint_set_P: the team's P upload failed");
    upload_tables(h);
 }
 
+// libgint_get_K: every thread completes its own queued work, then one thread copies the team's K
+// (collective, see Team). Threads that pass their own arrays get K in the array of the thread
+// that made the copy only, as in the reference.
 static void get_K_impl(Handle *h, double *Ka, double *Kb) {
    use_device(h);
    drain(h);
-   if (h->nspin == 0) { set_error(h, 4, "libgint_get_K before libgint_set_P"); return; }
-   double *dst[2] = {Ka, Kb};
-   for (int sp = 0; sp < h->nspin; sp++)
-      if (dst[sp]) ck(h, cudaMemcpy(dst[sp], h->d_K[sp].p, h->FP_size * 8, cudaMemcpyDeviceToHost), "K download");
+   const bool have = h->nspin != 0 && h->team && h->team->ok;
+   if (!have) set_error(h, 4, "libgint_get_K before libgint_set_P");
+   // every handle's kernels have finished adding into K
+#pragma omp barrier
+#pragma omp single
+   {
+      if (have) {
+         double *dst[2] = {Ka, Kb};
+         for (int sp = 0; sp < h->nspin; sp++)
+            if (dst[sp]) ck(h, cudaMemcpy(dst[sp], h->team->K[sp].p, h->FP_size * 8, cudaMemcpyDeviceToHost), "K download");
+      }
+   }
+}
+
+// libgint_set_K / libgint_set_K_polarized: collective like set_P; one thread uploads the team's K.
+static void set_K_impl(Handle *h, int nspin, const double *Ka, const double *Kb, int K_size) {
+   use_device(h);
+   const bool ok = h->nspin >= nspin && h->team && h->team->ok && (size_t)K_size == h->FP_size;
+   if (!ok) set_error(h, 2, nspin == 1 ? "libgint_set_K: call set_P first with the same size"
+                                       : "libgint_set_K_polarized: call set_P_polarized first");
+   drain(h);
+#pragma omp barrier
+#pragma omp single
+   {
+      if (ok) {
+         const double *src[2] = {Ka, Kb};
+         for (int sp = 0; sp < nspin; sp++) h2d(h, h->team->K[sp].p, src[sp], (size_t)K_size * 8, "K upload");
+         ck(h, cudaStreamSynchronize(h->stream), "K upload");
+      }
+   }
 }
 
 // Re-run every recorded batch with the current P (K is zeroed first). Returns the elapsed
@@ -670,7 +786,8 @@ static double replay_impl(Handle *h, double *kt, double *kcls = nullptr) {
    cudaEventCreate(&e0); cudaEventCreate(&e1);
    DevCtx ctx = make_ctx(h);
    ck(h, cudaEventRecord(e0, h->stream), "event");
-   for (int sp = 0; sp < h->nspin; sp++) ck(h, cudaMemsetAsync(h->d_K[sp].p, 0, h->FP_size * 8, h->stream), "K zero");
+   if (!h->team || !h->team->ok) { set_error(h, 4, "libgint_replay: call libgint_set_P first"); return -1.0; }
+   for (int sp = 0; sp < h->nspin; sp++) ck(h, cudaMemsetAsync(h->team->K[sp].p, 0, h->FP_size * 8, h->stream), "K zero");
    // optional per-kernel timing: one event pair per launch, summed per kernel
    std::vector<cudaEvent_t> kev;
    std::vector<int> kcl;
@@ -701,7 +818,8 @@ static double replay_impl(Handle *h, double *kt, double *kcls = nullptr) {
          bt.shells = (const ShellRec *)(base + g.o_sh);
          bt.groups = (const GroupRec *)(base + g.o_g);
          bt.qrtts = (const QrttRec *)(base + g.o_q);
-         bt.nprm = g.nprm; bt.nshell = g.nshell; bt.ngroup = g.ngroup;
+         bt.rowgrp = (const uint32_t *)(base + g.o_rg);
+         bt.nprm = g.nprm; bt.nshell = g.nshell; bt.ngroup = g.ngroup; bt.nqrtt = g.nqrtt;
          bt.AC = ac_half + g.ac_off;
          bt.gscratch = (double *)h->rec_gscr.p;
          int a_, b_;
@@ -778,6 +896,7 @@ void libgint_init(void *hh) {
       if (!h->work_ev[w]) ck(h, cudaEventCreateWithFlags(&h->work_ev[w], cudaEventDisableTiming), "event");
    }
    if (!h->fork_ev) ck(h, cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming), "event");
+   if (!h->noalloc_ev) ck(h, cudaEventCreateWithFlags(&h->noalloc_ev, cudaEventDisableTiming), "event");
    for (auto &row : h->batch_ev)
       for (cudaEvent_t &e : row)
          if (!e) ck(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
@@ -811,22 +930,9 @@ void libgint_set_P(void *hh, double *P, int P_size) { set_P_impl((Handle *)hh, 1
 
 void libgint_set_P_polarized(void *hh, double *Pa, double *Pb, int P_size) { set_P_impl((Handle *)hh, 2, Pa, Pb, P_size); }
 
-void libgint_set_K(void *hh, double *K, int K_size) {
-   Handle *h = (Handle *)hh;
-   if (h->nspin < 1 || (size_t)K_size != h->FP_size) { set_error(h, 2, "libgint_set_K: call set_P first with the same size"); return; }
-   drain(h);
-   h2d(h, h->d_K[0].p, K, (size_t)K_size * 8, "K upload");
-   ck(h, cudaStreamSynchronize(h->stream), "K upload");
-}
+void libgint_set_K(void *hh, double *K, int K_size) { set_K_impl((Handle *)hh, 1, K, nullptr, K_size); }
 
-void libgint_set_K_polarized(void *hh, double *Ka, double *Kb, int K_size) {
-   Handle *h = (Handle *)hh;
-   if (h->nspin < 2 || (size_t)K_size != h->FP_size) { set_error(h, 2, "libgint_set_K_polarized: call set_P_polarized first"); return; }
-   drain(h);
-   h2d(h, h->d_K[0].p, Ka, (size_t)K_size * 8, "K upload");
-   h2d(h, h->d_K[1].p, Kb, (size_t)K_size * 8, "K upload");
-   ck(h, cudaStreamSynchronize(h->stream), "K upload");
-}
+void libgint_set_K_polarized(void *hh, double *Ka, double *Kb, int K_size) { set_K_impl((Handle *)hh, 2, Ka, Kb, K_size); }
 
 void libgint_get_K(void *hh, double *K) { get_K_impl((Handle *)hh, K, nullptr); }
 
@@ -1211,9 +1317,11 @@ double libgint_replay(void *hh) { return replay_impl((Handle *)hh, nullptr); }
 // library's fixed device scratch (64 MiB) instead of buffers allocated by the handle. For
 // callers that cannot call cudaMalloc while building K. Every recorded class segment must fit
 // the scratch (record with a small libgint_set_max_mem, e.g. 150 MB, to keep batches small).
-// K_dev (K_size doubles) is zeroed and then accumulated on `stream` (the handle's stream if
-// null); the call returns after launching. Calls that overlap on the GPU share the scratch and
-// race. The first call on a device looks up the scratch address; make it before any stream
+// K_dev (K_size doubles, the P_size of the recorded build) is zeroed and then accumulated on
+// `stream` (the handle's stream if null), after the work already queued on the handle's stream
+// (the uploads of the recording); the call returns after launching. One density per call: a
+// spin-polarised caller makes one call per spin. Calls that overlap on the GPU share the scratch
+// and race. The first call on a device looks up the scratch address; make it before any stream
 // capture. Returns 0, or the handle's error code.
 int libgint_replay_noalloc(void *hh, const double *P_dev, double *K_dev, size_t K_size, void *stream) {
    Handle *h = (Handle *)hh;
@@ -1226,6 +1334,13 @@ int libgint_replay_noalloc(void *hh, const double *P_dev, double *K_dev, size_t 
       set_error(h, 2, "libgint_replay_noalloc: P_dev, K_dev and K_size must be given");
       return h->err;
    }
+   if (K_size != h->FP_size) {
+      set_error(h, 2, "libgint_replay_noalloc: K_size must be the P_size of the recorded K build");
+      return h->err;
+   }
+   // the handle's device holds the recording, the plans and the scratch this call uses
+   use_device(h);
+   if (h->err) return h->err;
    double *scr = nullptr;
    if (!ck(h, noalloc_scratch(&scr), "libgint_replay_noalloc: scratch lookup")) return h->err;
    // every class segment must fit: image-summed targets [nprm][S], then the HRR workspace
@@ -1246,6 +1361,12 @@ int libgint_replay_noalloc(void *hh, const double *P_dev, double *K_dev, size_t 
       }
    }
    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+   // the recorded batches' uploads (queued on the handle's stream by the recording build) come first
+   if (st != h->stream) {
+      if (!ck(h, cudaEventRecord(h->noalloc_ev, h->stream), "libgint_replay_noalloc: event record") ||
+          !ck(h, cudaStreamWaitEvent(st, h->noalloc_ev, 0), "libgint_replay_noalloc: stream wait"))
+         return h->err;
+   }
    DevCtx ctx = make_ctx(h);
    ctx.nspin = 1;
    ctx.P[0] = P_dev; ctx.P[1] = nullptr;
@@ -1266,7 +1387,8 @@ int libgint_replay_noalloc(void *hh, const double *P_dev, double *K_dev, size_t 
          bt.shells = (const ShellRec *)(base + g.o_sh);
          bt.groups = (const GroupRec *)(base + g.o_g);
          bt.qrtts = (const QrttRec *)(base + g.o_q);
-         bt.nprm = g.nprm; bt.nshell = g.nshell; bt.ngroup = g.ngroup;
+         bt.rowgrp = (const uint32_t *)(base + g.o_rg);
+         bt.nprm = g.nprm; bt.nshell = g.nshell; bt.ngroup = g.ngroup; bt.nqrtt = g.nqrtt;
          bt.AC = scr;                                                   // segments run in stream order
          bt.gscratch = scr + (((size_t)g.nprm * hp.S + 31) & ~(size_t)31);
          if (!ck(h, launch_prim(ctx, bt, hp, st), "libgint_replay_noalloc: k_prim launch")) return h->err;
@@ -1411,7 +1533,7 @@ const char *libgint_error_string(void *hh) { return ((Handle *)hh)->errmsg.c_str
 void libgint_destroy_handle(void *hh) {
    Handle *h = (Handle *)hh;
    if (!h) return;
-   if (h->stream) cudaStreamSynchronize(h->stream);
+   if (h->stream) { use_device(h); cudaStreamSynchronize(h->stream); }
    for (Slot &s : h->slots) {
       release(s.rec); release(s.ac); release(s.gscr);
       if (s.ev) cudaEventDestroy(s.ev);
@@ -1420,13 +1542,15 @@ void libgint_destroy_handle(void *hh) {
    for (auto &rb : h->recs) release(rb.rec);
    release(h->rec_ac); release(h->rec_gscr); release(h->d_cnt);
    DBuf *bufs[] = {&h->d_pool, &h->d_ents, &h->d_neighs, &h->d_C0, &h->d_lut, &h->d_bw, &h->d_ft, &h->d_vops,
-                   &h->d_plans, &h->d_err, &h->d_P[0], &h->d_P[1], &h->d_K[0], &h->d_K[1]};
+                   &h->d_plans, &h->d_err};
    for (DBuf *b : bufs) release(*b);
+   h->team.reset();
    for (int w = 0; w < kWorkStreams; w++) {
       if (h->work[w]) cudaStreamDestroy(h->work[w]);
       if (h->work_ev[w]) cudaEventDestroy(h->work_ev[w]);
    }
    if (h->fork_ev) cudaEventDestroy(h->fork_ev);
+   if (h->noalloc_ev) cudaEventDestroy(h->noalloc_ev);
    for (auto &row : h->batch_ev)
       for (cudaEvent_t e : row)
          if (e) cudaEventDestroy(e);

@@ -1,11 +1,11 @@
 // group3.cu -- k_group3<la,lb,lc,ld>: contraction + HRR + image-pair sum + spherical transform +
-// K update, one lane per group, for the classes with generated HRR code (grp_gen.cuh).
+// K update, one lane per contraction row, for the classes with generated HRR code (grp_gen.cuh).
 //
 // A group is one set quartet of one class: all its image pairs (shell quartets) and its
-// nla*nlb*nlc*nld contraction rows. For every row the lane contracts the image-summed targets of
-// each shell over its primitives, applies that shell's HRR (its own AB and CD), sums the shells,
-// transforms the sum to spherical harmonics and adds the four exchange updates to K with
-// atomics (reference src/compute_ECO.cpp:12-214, src/compute_HRR.cpp:102-225,
+// nla*nlb*nlc*nld contraction rows. One lane takes one row: it contracts the image-summed targets
+// of each shell over its primitives with the row's coefficients, applies that shell's HRR (its own
+// AB and CD), sums the shells, transforms the sum to spherical harmonics and adds the four exchange
+// updates to K with atomics (reference src/compute_ECO.cpp:12-214, src/compute_HRR.cpp:102-225,
 // src/compute_SPH.cpp:58-237, src/compute_KS.cpp:8-117). All indices are compile-time
 // constants and the workspace lives in registers.
 //
@@ -46,68 +46,74 @@ __global__ void __launch_bounds__(128, Group3Shape<LA, LB, LC, LD>::MINB) k_grou
    constexpr int S = G::S, Nc = G::Nc, Ns = G::Ns;
    constexpr int nsb = 2 * LB + 1, nsc = 2 * LC + 1, nsd = 2 * LD + 1;
    constexpr int nscd = nsc * nsd, nsbcd = nsb * nscd;
-   for (uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x; gi < bt.ngroup; gi += gridDim.x * blockDim.x) {
+   const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+   const uint32_t nblk = (bt.nqrtt + 31) >> 5;
+   // one lane per contraction row: a warp takes 32 consecutive rows, so the lanes of one set
+   // quartet's rows read the same primitive codes and image-summed targets (broadcast loads)
+   for (uint32_t blk = blockIdx.x * wpb + (threadIdx.x >> 5); blk < nblk; blk += gridDim.x * wpb) {
+      const uint32_t q0 = blk << 5, q = q0 + lane;
+      const uint32_t gi = row_group_warp(bt, q0, lane);
+      if (q >= bt.nqrtt) continue;
       const GroupRec Gr = bt.groups[gi];
       const int nl1 = Gr.nl[1], nl2 = Gr.nl[2], nl3 = Gr.nl[3];
-      const int nlabcd = Gr.nl[0] * nl1 * nl2 * nl3;
-      for (int r = 0; r < nlabcd; r++) {
-         const int ia = r / (nl1 * nl2 * nl3), ib = (r / (nl2 * nl3)) % nl1, ic = (r / nl3) % nl2, id = r % nl3;
-         double cart[Nc];
+      const int r = (int)(q - Gr.qrtt_off);
+      const int ia = r / (nl1 * nl2 * nl3), ib = (r / (nl2 * nl3)) % nl1, ic = (r / nl3) % nl2, id = r % nl3;
+      double cart[Nc];
 #pragma unroll
-         for (int q = 0; q < Nc; q++) cart[q] = 0.0;
-         for (uint32_t s = 0; s < Gr.nshell; s++) {
-            const ShellRec sh = bt.shells[Gr.shell_off + s];
-            const BasisEnt ea = ctx.ents[sh.ent[0]], eb = ctx.ents[sh.ent[1]];
-            const BasisEnt ec = ctx.ents[sh.ent[2]], ed = ctx.ents[sh.ent[3]];
-            const double *Ka = ctx.pool + ea.k_off + ia * ea.np;
-            const double *Kb = ctx.pool + eb.k_off + ib * eb.np;
-            const double *Kc = ctx.pool + ec.k_off + ic * ec.np;
-            const double *Kd = ctx.pool + ed.k_off + id * ed.np;
-            double T[S];
+      for (int t = 0; t < Nc; t++) cart[t] = 0.0;
+      for (uint32_t s = 0; s < Gr.nshell; s++) {
+         const ShellRec sh = bt.shells[Gr.shell_off + s];
+         const BasisEnt ea = ctx.ents[sh.ent[0]], eb = ctx.ents[sh.ent[1]];
+         const BasisEnt ec = ctx.ents[sh.ent[2]], ed = ctx.ents[sh.ent[3]];
+         const double *Ka = ctx.pool + ea.k_off + ia * ea.np;
+         const double *Kb = ctx.pool + eb.k_off + ib * eb.np;
+         const double *Kc = ctx.pool + ec.k_off + ic * ec.np;
+         const double *Kd = ctx.pool + ed.k_off + id * ed.np;
+         double T[S];
 #pragma unroll
-            for (int j = 0; j < S; j++) T[j] = 0.0;
-            // two primitives per iteration so that the next one's loads overlap this one's FMAs
+         for (int j = 0; j < S; j++) T[j] = 0.0;
+         // contraction over the primitives (reference src/compute_ECO.cpp:131-212); two per
+         // iteration so that the next one's loads overlap this one's FMAs
 #pragma unroll 2
-            for (uint32_t ip = 0; ip < sh.nprm; ip++) {
-               const uint32_t code = __ldg(bt.prm + sh.prm_off + ip);
-               const double kp = __ldg(Ka + (code >> 24)) * __ldg(Kb + ((code >> 16) & 255)) *
-                                 __ldg(Kc + ((code >> 8) & 255)) * __ldg(Kd + (code & 255));
-               const double *row = bt.AC + (size_t)(sh.prm_off + ip) * S;
+         for (uint32_t ip = 0; ip < sh.nprm; ip++) {
+            const uint32_t code = __ldg(bt.prm + sh.prm_off + ip);
+            const double kp = __ldg(Ka + (code >> 24)) * __ldg(Kb + ((code >> 16) & 255)) *
+                              __ldg(Kc + ((code >> 8) & 255)) * __ldg(Kd + (code & 255));
+            const double *row = bt.AC + (size_t)(sh.prm_off + ip) * S;
 #pragma unroll
-               for (int j = 0; j < S; j++) T[j] += kp * __ldg(row + j);
-            }
-            double A[3], B[3], C[3], D[3], CDs[3];
-            shell_geom(ctx, ea, eb, ec, ed, sh.n1, sh.n2, A, B, C, D, CDs);
-            const double AB[3] = {A[0] - B[0], A[1] - B[1], A[2] - B[2]};
-            const double CD[3] = {C[0] - D[0], C[1] - D[1], C[2] - D[2]};
-            G::hrr(T, AB, CD, cart);
+            for (int j = 0; j < S; j++) T[j] += kp * __ldg(row + j);
          }
-         double sph[Ns];
-         G::sph(cart, sph);
-         const QrttRec k = bt.qrtts[Gr.qrtt_off + r];
-         const double fac = symm_factor(k.idx_fac) * ctx.hf_fac;
+         double A[3], B[3], C[3], D[3], CDs[3];
+         shell_geom(ctx, ea, eb, ec, ed, sh.n1, sh.n2, A, B, C, D, CDs);
+         const double AB[3] = {A[0] - B[0], A[1] - B[1], A[2] - B[2]};
+         const double CD[3] = {C[0] - D[0], C[1] - D[1], C[2] - D[2]};
+         G::hrr(T, AB, CD, cart);
+      }
+      double sph[Ns];
+      G::sph(cart, sph);
+      const QrttRec k = bt.qrtts[q];
+      const double fac = symm_factor(k.idx_fac) * ctx.hf_fac;
 #pragma unroll
-         for (int t = 0; t < Ns; t++) {
-            const int isa = t / nsbcd, isb = (t / nscd) % nsb, isc = (t / nsd) % nsc, isd = t % nsd;
-            const int iac = !(k.T & 1) ? isc * k.ld[0] + isa : isa * k.ld[0] + isc;
-            const int iad = !(k.T & 2) ? isd * k.ld[1] + isa : isa * k.ld[1] + isd;
-            const int ibc = !(k.T & 4) ? isc * k.ld[2] + isb : isb * k.ld[2] + isc;
-            const int ibd = !(k.T & 8) ? isd * k.ld[3] + isb : isb * k.ld[3] + isd;
-            const size_t Iac = (size_t)k.off[0] + iac, Iad = (size_t)k.off[1] + iad;
-            const size_t Ibc = (size_t)k.off[2] + ibc, Ibd = (size_t)k.off[3] + ibd;
-            if (Iac >= ctx.FP_size || Iad >= ctx.FP_size || Ibc >= ctx.FP_size || Ibd >= ctx.FP_size) {
-               atomicOr(ctx.err, 1);
-               continue;
-            }
-            const double iabcd = -fac * sph[t];
-            for (int sp = 0; sp < ctx.nspin; sp++) {
-               const double *Pm = ctx.P[sp];
-               double *Km = ctx.K[sp];
-               atomicAdd(Km + Ibd, iabcd * __ldg(Pm + Iac));
-               atomicAdd(Km + Ibc, iabcd * __ldg(Pm + Iad));
-               atomicAdd(Km + Iad, iabcd * __ldg(Pm + Ibc));
-               atomicAdd(Km + Iac, iabcd * __ldg(Pm + Ibd));
-            }
+      for (int t = 0; t < Ns; t++) {
+         const int isa = t / nsbcd, isb = (t / nscd) % nsb, isc = (t / nsd) % nsc, isd = t % nsd;
+         const int iac = !(k.T & 1) ? isc * k.ld[0] + isa : isa * k.ld[0] + isc;
+         const int iad = !(k.T & 2) ? isd * k.ld[1] + isa : isa * k.ld[1] + isd;
+         const int ibc = !(k.T & 4) ? isc * k.ld[2] + isb : isb * k.ld[2] + isc;
+         const int ibd = !(k.T & 8) ? isd * k.ld[3] + isb : isb * k.ld[3] + isd;
+         const size_t Iac = (size_t)k.off[0] + iac, Iad = (size_t)k.off[1] + iad;
+         const size_t Ibc = (size_t)k.off[2] + ibc, Ibd = (size_t)k.off[3] + ibd;
+         if (Iac >= ctx.FP_size || Iad >= ctx.FP_size || Ibc >= ctx.FP_size || Ibd >= ctx.FP_size) {
+            atomicOr(ctx.err, 1);
+            continue;
+         }
+         const double iabcd = -fac * sph[t];
+         for (int sp = 0; sp < ctx.nspin; sp++) {
+            const double *Pm = ctx.P[sp];
+            double *Km = ctx.K[sp];
+            atomicAdd(Km + Ibd, iabcd * __ldg(Pm + Iac));
+            atomicAdd(Km + Ibc, iabcd * __ldg(Pm + Iad));
+            atomicAdd(Km + Iad, iabcd * __ldg(Pm + Ibc));
+            atomicAdd(Km + Iac, iabcd * __ldg(Pm + Ibd));
          }
       }
    }
@@ -116,7 +122,7 @@ __global__ void __launch_bounds__(128, Group3Shape<LA, LB, LC, LD>::MINB) k_grou
 template <int LA, int LB, int LC, int LD>
 cudaError_t launch_one(const DevCtx &ctx, const BatchArgs &bt, cudaStream_t st) {
    const int threads = 128;
-   const long blocks = std::max(1L, std::min(((long)bt.ngroup + threads - 1) / threads, 148L * 16));
+   const long blocks = std::max(1L, std::min(((long)bt.nqrtt + threads - 1) / threads, 148L * 16));
    k_group3<LA, LB, LC, LD><<<(unsigned)blocks, threads, 0, st>>>(ctx, bt);
    return cudaGetLastError();
 }
@@ -159,7 +165,7 @@ struct PartPreload {
 #define GROUP3_CAT(a, b) GROUP3_CAT2(a, b)
 bool GROUP3_CAT(group3_launch_part, GROUP3_PART)(const DevCtx &ctx, const BatchArgs &bt, cudaStream_t st,
                                                  cudaError_t *err) {
-   if (bt.ngroup == 0) { *err = cudaSuccess; return true; }
+   if (bt.nqrtt == 0) { *err = cudaSuccess; return true; }
    return PartTable<GROUP3_PART>::launch(bt.cls, ctx, bt, st, err);
 }
 

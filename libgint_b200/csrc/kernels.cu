@@ -172,9 +172,9 @@ __global__ void __launch_bounds__(256) k_prim(DevCtx ctx, BatchArgs bt, int team
                const double g0 = __ldg(ctx.neighs + n3s * 3 + 0), g1 = __ldg(ctx.neighs + n3s * 3 + 1),
                             g2 = __ldg(ctx.neighs + n3s * 3 + 2);
                const double Qp0 = g.Q[0] + g0, Qp1 = g.Q[1] + g1, Qp2 = g.Q[2] + g2;
-               const double W0 = (g.zab * g.P[0] + g.zcd * Qp0) * g.inv_z;
-               const double W1 = (g.zab * g.P[1] + g.zcd * Qp1) * g.inv_z;
-               const double W2 = (g.zab * g.P[2] + g.zcd * Qp2) * g.inv_z;
+               const double W0 = wdist(g.zab, g.P[0], g.zcd, Qp0, g.inv_z);
+               const double W1 = wdist(g.zab, g.P[1], g.zcd, Qp1, g.inv_z);
+               const double W2 = wdist(g.zab, g.P[2], g.zcd, Qp2, g.inv_z);
                pqz[0] = g.PA[0]; pqz[1] = g.PA[1]; pqz[2] = g.PA[2];
                pqz[3] = W0 - g.P[0]; pqz[4] = W1 - g.P[1]; pqz[5] = W2 - g.P[2];
                pqz[6] = g.QC[0]; pqz[7] = g.QC[1]; pqz[8] = g.QC[2];
@@ -296,7 +296,7 @@ __global__ void __launch_bounds__(256) k_prim2(DevCtx ctx, BatchArgs bt, int cp,
                const double Qp[3] = {g.Q[0] + g0, g.Q[1] + g1, g.Q[2] + g2};
                double *pz = pqz + lane;
                for (int q = 0; q < 3; q++) {
-                  const double W = (g.zab * g.P[q] + g.zcd * Qp[q]) * g.inv_z;
+                  const double W = wdist(g.zab, g.P[q], g.zcd, Qp[q], g.inv_z);
                   pz[q * 32] = g.PA[q];
                   pz[(3 + q) * 32] = W - g.P[q];
                   pz[(6 + q) * 32] = g.QC[q];
@@ -329,7 +329,7 @@ __global__ void __launch_bounds__(256) k_prim2(DevCtx ctx, BatchArgs bt, int cp,
                   const int q = lane;
                   const double gq = __ldg(ctx.neighs + n3 * 3 + q);
                   const double Qp = g.Q[q] + gq;
-                  const double W = (g.zab * g.P[q] + g.zcd * Qp) * g.inv_z;
+                  const double W = wdist(g.zab, g.P[q], g.zcd, Qp, g.inv_z);
                   pqz[q] = g.PA[q]; pqz[3 + q] = W - g.P[q]; pqz[6 + q] = g.QC[q]; pqz[9 + q] = W - Qp;
                } else if (lane == 3) {
                   pqz[12] = g.i2ab; pqz[13] = g.mrab; pqz[14] = g.i2cd; pqz[15] = g.mrcd; pqz[16] = g.i2z;
@@ -501,17 +501,18 @@ static __device__ __forceinline__ void sph_pass(const double *src, double *dst, 
 // q = t / n for t * n < 2^20, with M = 2^20 / n + 1 (all spherical indices here: t < 7^4, n <= 7^3)
 static __device__ __forceinline__ int div_small(int t, uint32_t M) { return (int)(((uint32_t)t * M) >> 20); }
 
+// One contraction row q (of group G) processed by NL cooperating lanes.
 template <int NL, int ST>
 static __device__ __forceinline__ void group_body(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan *pl,
-                                                  const GroupRec &G, double *ws, double *cart, int lane,
+                                                  const GroupRec &G, uint32_t q, double *ws, double *cart, int lane,
                                                   const uint2 *hrec, double *kpw) {
    const int S = pl->S, Nc = pl->Nc, Ns = pl->Ns;
    const int la = pl->la, lb = pl->lb, lc = pl->lc, ld = pl->ld;
    const int nca = ncart(la), ncb = ncart(lb), ncc = ncart(lc), ncd_ = ncart(ld);
    const int nsa = 2 * la + 1, nsb = 2 * lb + 1, nsc = 2 * lc + 1, nsd = 2 * ld + 1;
    const int nl1 = G.nl[1], nl2 = G.nl[2], nl3 = G.nl[3];
-   const int nlabcd = G.nl[0] * nl1 * nl2 * nl3;
-   for (int r = 0; r < nlabcd; r++) {
+   {
+      const int r = (int)(q - G.qrtt_off);
       const int ia = r / (nl1 * nl2 * nl3), ib = (r / (nl2 * nl3)) % nl1, ic = (r / nl3) % nl2, id = r % nl3;
       for (int q = lane; q < Nc; q += NL) cart[q * ST] = 0.0;
       for (uint32_t s = 0; s < G.nshell; s++) {
@@ -620,7 +621,7 @@ static __device__ __forceinline__ void group_body(const DevCtx &ctx, const Batch
          }
       }
       // K update (reference src/compute_KS.cpp:26-115)
-      const QrttRec k = bt.qrtts[G.qrtt_off + r];
+      const QrttRec k = bt.qrtts[q];
       const double fac = c_symm[k.idx_fac] * ctx.hf_fac;
       const int nscd = nsc * nsd, nsbcd = nsb * nscd;
       const uint32_t Mbcd = (1u << 20) / nsbcd + 1, Mcd = (1u << 20) / nscd + 1, Md = (1u << 20) / nsd + 1;
@@ -661,7 +662,7 @@ static __device__ __forceinline__ void load_plan(const ClassPlan *src_plan, doub
    for (int w = threadIdx.x; w < nwords; w += blockDim.x) dst[w] = src[w];
 }
 
-// one warp per group
+// one warp per contraction row
 __global__ void __launch_bounds__(256) k_group(DevCtx ctx, BatchArgs bt, int warp_doubles, int use_global) {
    extern __shared__ __align__(16) double smem[];
    const ClassPlan *pl = reinterpret_cast<const ClassPlan *>(smem);
@@ -676,13 +677,13 @@ __global__ void __launch_bounds__(256) k_group(DevCtx ctx, BatchArgs bt, int war
                               : (smem + plan_doubles + nwarp * kGroupKpDoubles + (size_t)warp * warp_doubles);
    const int Hws = max(pl->H, 2 * pl->Nc);
    const uint2 *hrec = ctx.gprog + ctx.gprog[bt.cls].x;
-   for (uint32_t g = gwarp; g < bt.ngroup; g += gridDim.x * nwarp) {
-      const GroupRec G = bt.groups[g];
-      group_body<32, 1>(ctx, bt, pl, G, wbase, wbase + Hws, lane, hrec, kpw);
+   for (uint32_t q = gwarp; q < bt.nqrtt; q += gridDim.x * nwarp) {
+      const GroupRec G = bt.groups[row_group_one(bt, q, lane)];
+      group_body<32, 1>(ctx, bt, pl, G, q, wbase, wbase + Hws, lane, hrec, kpw);
    }
 }
 
-// one lane per group, for classes with a small workspace (lane-interleaved in shared memory)
+// one lane per contraction row, for classes with a small workspace (lane-interleaved in shared memory)
 __global__ void __launch_bounds__(256) k_group_lane(DevCtx ctx, BatchArgs bt, int lane_doubles) {
    extern __shared__ __align__(16) double smem[];
    const ClassPlan *pl = reinterpret_cast<const ClassPlan *>(smem);
@@ -693,11 +694,14 @@ __global__ void __launch_bounds__(256) k_group_lane(DevCtx ctx, BatchArgs bt, in
    double *wbase = smem + plan_doubles + (size_t)warp * 32 * lane_doubles + lane;
    const int Hws = max(pl->H, 2 * pl->Nc);
    const uint2 *hrec = ctx.gprog + ctx.gprog[bt.cls].x;
-   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < bt.ngroup; g += gridDim.x * blockDim.x) {
-      const GroupRec G = bt.groups[g];
-      group_body<1, 32>(ctx, bt, pl, G, wbase, wbase + Hws * 32, 0, hrec, nullptr);
+   const uint32_t nblk = (bt.nqrtt + 31) >> 5;
+   for (uint32_t blk = blockIdx.x * nwarp + warp; blk < nblk; blk += gridDim.x * nwarp) {
+      const uint32_t q0 = blk << 5, q = q0 + lane;
+      const uint32_t gi = row_group_warp(bt, q0, lane);
+      if (q >= bt.nqrtt) continue;
+      const GroupRec G = bt.groups[gi];
+      group_body<1, 32>(ctx, bt, pl, G, q, wbase, wbase + Hws * 32, 0, hrec, nullptr);
    }
-   (void)nwarp;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -847,19 +851,14 @@ static bool prim2_lane(const ClassPlan &hp) { return hp.V <= 96; }
 
 
 // Primitive-kernel choice: k_prim3 (generated VRR) for the classes it covers, then k_prim2,
-// then the team kernel for the largest classes. LIBGINT_PRIM_KERNEL=2 skips k_prim3 and =1 uses
-// the team kernel only (for comparisons).
+// then the team kernel for the largest classes.
 cudaError_t launch_prim(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan &hp, cudaStream_t st) {
    if (bt.nprm == 0) return cudaSuccess;
-   static const int prim_kernel = [] {
-      const char *e = getenv("LIBGINT_PRIM_KERNEL");
-      return (e && e[0] == '1') ? 1 : ((e && e[0] == '2') ? 2 : 3);
-   }();
-   if (prim_kernel == 3) {
+   {
       cudaError_t err = cudaSuccess;
       if (prim3_launch(ctx, bt, st, &err)) return err;
    }
-   if (prim_kernel >= 2) {
+   {
       const bool lane = prim2_lane(hp);
       int cp = 1;
       size_t wd = 0;
@@ -914,14 +913,10 @@ size_t group_global_scratch(const ClassPlan &hp, int *grid, int *warps) {
 
 
 // Group-kernel choice: k_group3 (generated HRR, one lane per group) for the classes it covers,
-// then k_group_lane / k_group. LIBGINT_GROUP_KERNEL=2 skips k_group3 (for comparisons).
+// then k_group_lane / k_group.
 cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan &hp, cudaStream_t st) {
-   if (bt.ngroup == 0) return cudaSuccess;
-   static const int group_kernel = [] {
-      const char *e = getenv("LIBGINT_GROUP_KERNEL");
-      return (e && e[0] == '2') ? 2 : 3;
-   }();
-   if (group_kernel == 3) {
+   if (bt.nqrtt == 0) return cudaSuccess;
+   {
       cudaError_t err = cudaSuccess;
       if (group3_launch(ctx, bt, st, &err)) return err;
    }
@@ -932,7 +927,7 @@ cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan
       const size_t plan_bytes = group_hdr_bytes();
       const int nw = 8;
       const size_t smem = plan_bytes + (size_t)nw * 32 * lane_doubles * 8;
-      long blocks = ((long)bt.ngroup + nw * 32 - 1) / (nw * 32);
+      long blocks = ((long)bt.nqrtt + nw * 32 - 1) / (nw * 32);
       blocks = std::max(1L, std::min(blocks, 148L * 16));
       k_group_lane<<<(unsigned)blocks, nw * 32, smem, st>>>(ctx, bt, lane_doubles);
       return cudaGetLastError();
@@ -941,7 +936,7 @@ cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan
    const int nw = group_smem_warps(wd);
    if (nw >= 1) {
       const size_t smem = plan_bytes + (size_t)nw * (wd + kGroupKpDoubles) * 8;
-      long blocks = ((long)bt.ngroup + nw - 1) / nw;
+      long blocks = ((long)bt.nqrtt + nw - 1) / nw;
       blocks = std::max(1L, std::min(blocks, 148L * 64));
       k_group<<<(unsigned)blocks, nw * 32, smem, st>>>(ctx, bt, (int)wd, 0);
    } else {

@@ -53,6 +53,8 @@ struct BatchArgs {
    const GroupRec *groups;
    const QrttRec *qrtts;
    uint32_t nprm, nshell, ngroup;
+   uint32_t nqrtt;            // contraction rows (the group kernels' work items), in group order
+   const uint32_t *rowgrp;    // group of row 32 k, k < (nqrtt + 31) / 32
    double *AC;                // [nprm][S] image-summed VRR targets
    double *gscratch;          // HRR workspace in global memory for the largest classes
    int cls;                   // la*64 + lb*16 + lc*4 + ld

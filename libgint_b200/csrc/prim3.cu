@@ -132,7 +132,7 @@ k_prim3(DevCtx ctx, BatchArgs bt) {
 #pragma unroll
          for (int q = 0; q < 3; q++) {
             const double Qp = g.Q[q] + sneigh[n3 * 3 + q];
-            const double W = (g.zab * g.P[q] + g.zcd * Qp) * g.inv_z;
+            const double W = wdist(g.zab, g.P[q], g.zcd, Qp, g.inv_z);
             z[q] = g.PA[q];
             z[3 + q] = W - g.P[q];
             z[6 + q] = g.QC[q];

@@ -300,4 +300,30 @@ static __device__ __forceinline__ int fm_eval_geo(const DevCtx &ctx, int L_rt, c
    return 1;
 }
 
+// ---------------------------------------------------------------------------------------
+// Contraction rows (QrttRec) are the group kernels' work items; rows are stored in group order,
+// group g owning rows [qrtt_off, qrtt_off + nla nlb nlc nld). bt.rowgrp[q / 32] is the group of
+// row 32 (q / 32), and at most 32 groups start within one 32-row block.
+// ---------------------------------------------------------------------------------------
+// the group of row q0 + lane for every lane of a converged warp (q0 a multiple of 32)
+static __device__ __forceinline__ uint32_t row_group_warp(const BatchArgs &bt, uint32_t q0, int lane) {
+   const uint32_t g0 = __ldg(bt.rowgrp + (q0 >> 5));
+   const uint32_t gi = g0 + (uint32_t)lane;
+   unsigned bit = 0;
+   if (lane > 0 && gi < bt.ngroup) {
+      const uint32_t st = __ldg(&bt.groups[gi].qrtt_off);   // > q0: group g0 holds row q0
+      if (st - q0 < 32u) bit = 1u << (st - q0);
+   }
+   const unsigned M = __reduce_or_sync(0xffffffffu, bit);
+   return g0 + __popc(M & ((2u << lane) - 1u));
+}
+
+// the group of row q, the same in every lane of a converged warp
+static __device__ __forceinline__ uint32_t row_group_one(const BatchArgs &bt, uint32_t q, int lane) {
+   const uint32_t g0 = __ldg(bt.rowgrp + (q >> 5));
+   const uint32_t gi = g0 + 1u + (uint32_t)lane;
+   const bool later = gi < bt.ngroup && __ldg(&bt.groups[gi].qrtt_off) <= q;
+   return g0 + __popc(__ballot_sync(0xffffffffu, later));
+}
+
 }  // namespace gint

@@ -17,8 +17,8 @@ decimals); tests/test_grp_gen.py checks them bit for bit against libgint_host_ta
 Output per class with L = la+lb+lc+ld <= LGMAX and an HRR workspace of at most HMAX doubles:
   template <> struct GrpGen<la, lb, lc, ld> {
      static constexpr bool kHas = true; static constexpr int S, Nc, Ns;
-     static __device__ void hrr(const double *T, const double *AB, const double *CD, double *cart);  // cart += ...
-     static __device__ void sph(const double *cart, double *out);
+     template <class R> static __device__ void hrr(const R *T, const R *AB, const R *CD, R *cart);  // cart += ...
+     template <class R> static __device__ void sph(const R *cart, R *out);
   };
 
 Run:  python -m libgint_b200.gen_grp     (rewrites csrc/grp_gen.cuh)
@@ -139,7 +139,7 @@ def gen_class(la, lb, lc, ld):
                         lm = cidx(lowered(ed, t))
                         kp = cidx(_inc(cart(c, k), t))
                         n = f"k{c}_{d}_{x}_{k}_{l}"
-                        lines.append(f"      const double {n} = {K[(c + 1, d - 1, x, kp, lm)]} + CD[{t}] * "
+                        lines.append(f"      const R {n} = {K[(c + 1, d - 1, x, kp, lm)]} + CD[{t}] * "
                                      f"{K[(c, d - 1, x, k, lm)]};")
                         K[(c, d, x, k, l)] = n
     ncd = ncart(lc) * ncart(ld)
@@ -160,7 +160,7 @@ def gen_class(la, lb, lc, ld):
                     ip = cidx(_inc(cart(a, i), t))
                     for q in range(ncd):
                         n = f"b{a}_{b}_{i}_{j}_{q}"
-                        lines.append(f"      const double {n} = {Bv[(a + 1, b - 1, ip, jm, q)]} + AB[{t}] * "
+                        lines.append(f"      const R {n} = {Bv[(a + 1, b - 1, ip, jm, q)]} + AB[{t}] * "
                                      f"{Bv[(a, b - 1, i, jm, q)]};")
                         Bv[(a, b, i, j, q)] = n
     nca, ncb = ncart(la), ncart(lb)
@@ -200,8 +200,8 @@ def gen_class(la, lb, lc, ld):
                 continue
             terms = [(cc[mi][k], cur[base + k * stride]) for k in range(dims[ctr]) if cc[mi][k] != 0.0]
             n = f"s{ctr}_{t}"
-            expr = " + ".join(f"{repr(float(v))} * {x}" for v, x in terms) if terms else "0.0"
-            slines.append(f"      const double {n} = {expr};")
+            expr = " + ".join(f"R({repr(float(v))}) * {x}" for v, x in terms) if terms else "R(0)"
+            slines.append(f"      const R {n} = {expr};")
             nxt[t] = n
         cur = nxt
         dims = nd
@@ -216,12 +216,13 @@ def gen_class(la, lb, lc, ld):
         f"struct GrpGen<{la}, {lb}, {lc}, {ld}> {{",
         "   static constexpr bool kHas = true;",
         f"   static constexpr int S = {p['S']}, Nc = {Nc}, Ns = {Ns};",
-        "   static __device__ __forceinline__ void hrr(const double *__restrict__ T, const double *AB, const double *CD,",
-        "                                              double *cart) {",
+        "   template <class R>",
+        "   static __device__ __forceinline__ void hrr(const R *__restrict__ T, const R *AB, const R *CD, R *cart) {",
         hrr_body,
         "      (void)AB; (void)CD;",
         "   }",
-        "   static __device__ __forceinline__ void sph(const double *cart, double *out) {",
+        "   template <class R>",
+        "   static __device__ __forceinline__ void sph(const R *cart, R *out) {",
         sph_body,
         "   }",
         "};",

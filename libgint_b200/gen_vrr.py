@@ -19,7 +19,7 @@ axis on which the cartesian function has a nonzero exponent, "-1_d" lowers that 
 Output: for every class with at most VMAX workspace elements, a specialisation
   template <> struct VrrGen<la, lb, lc, ld> {
      static constexpr bool kHas = true; static constexpr int S, s00;
-     template <class Out> static __device__ void run(const double *F, const double *z, Out &out);
+     template <class R, class Out> static __device__ void run(const R *F, const R *z, Out &out);
   };
 where F holds (0|0)^(m), m = 0..L, and out(s, v) receives target element s of the contracted-
 target layout (one panel per ket shell f over every bra cartesian e, as csrc/plan.cpp). The
@@ -115,7 +115,7 @@ def plan(la, lb, lc, ld):
 
 
 def _num(x):
-    return f"{float(x):.1f}"
+    return f"R({float(x):.1f})"
 
 
 def gen_class(la, lb, lc, ld, vreg=VREG):
@@ -123,7 +123,7 @@ def gen_class(la, lb, lc, ld, vreg=VREG):
     if p["V"] <= vreg:
         # named values: the compiler keeps the live ones in registers
         name = lambda a, c, i, k, m: f"x{a}_{c}_{i}_{k}_{m}"
-        decl = "const double "
+        decl = "const R "
     else:
         # one per-lane array with compile-time indices (too many values for registers; this also
         # keeps the register allocator's work linear in the number of elements)
@@ -137,7 +137,7 @@ def gen_class(la, lb, lc, ld, vreg=VREG):
                         o += 1
         name = lambda a, c, i, k, m: f"w[{off[(a, c, i, k, m)]}]"
         decl = ""
-    lines = [] if p["V"] <= vreg else [f"      double w[{p['V']}];"]
+    lines = [] if p["V"] <= vreg else [f"      R w[{p['V']}];"]
     for a, c, l0, h0 in p["blocks"]:
         for m in range(l0, h0 + 1):
             for i in range(ncart(a)):
@@ -190,13 +190,13 @@ def gen_class(la, lb, lc, ld, vreg=VREG):
         f"   static constexpr int S = {p['S']};",
         f"   static constexpr int s00 = {s00};",
         f"   static constexpr int nout = {len(outs)};",
-        "   template <class Out>",
-        "   static __device__ __forceinline__ void run(const double *__restrict__ F, const double *__restrict__ z, Out &out) {",
+        "   template <class R, class Out>",
+        "   static __device__ __forceinline__ void run(const R *__restrict__ F, const R *__restrict__ z, Out &out) {",
     ]
     if p["V"] > 1:
-        head.append("      const double PA0 = z[0], PA1 = z[1], PA2 = z[2], WP0 = z[3], WP1 = z[4], WP2 = z[5];")
-        head.append("      const double QC0 = z[6], QC1 = z[7], QC2 = z[8], WQ0 = z[9], WQ1 = z[10], WQ2 = z[11];")
-        head.append("      const double i2ab = z[12], mrab = z[13], i2cd = z[14], mrcd = z[15], i2z = z[16];")
+        head.append("      const R PA0 = z[0], PA1 = z[1], PA2 = z[2], WP0 = z[3], WP1 = z[4], WP2 = z[5];")
+        head.append("      const R QC0 = z[6], QC1 = z[7], QC2 = z[8], WQ0 = z[9], WQ1 = z[10], WQ2 = z[11];")
+        head.append("      const R i2ab = z[12], mrab = z[13], i2cd = z[14], mrcd = z[15], i2z = z[16];")
     tail = [f"      out({s}, {n});" for s, n in outs]
     unused = ("      (void)PA0; (void)PA1; (void)PA2; (void)WP0; (void)WP1; (void)WP2; (void)QC0; (void)QC1;"
               " (void)QC2; (void)WQ0; (void)WQ1; (void)WQ2; (void)i2ab; (void)mrab; (void)i2cd; (void)mrcd;"

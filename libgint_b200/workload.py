@@ -24,7 +24,8 @@ class GdConfig(ctypes.Structure):
                 ("n_img_1d", ctypes.c_int), ("basis", ctypes.c_int), ("n_occ", ctypes.c_int),
                 ("rc_ang", ctypes.c_double), ("eps_schwarz", ctypes.c_double),
                 ("seed", ctypes.c_uint64), ("full_enum", ctypes.c_int), ("max_prm", ctypes.c_int),
-                ("max_ncontr", ctypes.c_int)]
+                ("max_ncontr", ctypes.c_int), ("setq_stride", ctypes.c_int), ("setq_phase", ctypes.c_int),
+                ("threads", ctypes.c_int)]
 
 
 class GdInfo(ctypes.Structure):
@@ -77,6 +78,9 @@ def driver():
         lib.gd_build_K_mt.restype = ctypes.c_double
         lib.gd_build_K_mt.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
                                       _D, _D, ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_long), _D]
+        lib.gd_build_K_team.restype = ctypes.c_double
+        lib.gd_build_K_team.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
+                                        _D, _D, ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_long), _D]
         lib.gd_mt_split.restype = None
         lib.gd_mt_split.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_long), ctypes.c_long, ctypes.c_int,
                                     ctypes.POINTER(ctypes.c_long)]
@@ -101,17 +105,20 @@ class Workload:
     """A generated system plus its screened add_* call stream."""
 
     def __init__(self, name=None, seed=0, eps_schwarz=1e-11, rc_ang=6.0, full_enum=False,
-                 max_prm=16, max_ncontr=4, **overrides):
+                 max_prm=16, max_ncontr=4, setq_stride=1, setq_phase=0, threads=0, **overrides):
         params = dict(CONFIGS[name]) if name else {}
         params.update(overrides)
         cfg = GdConfig(n_mol=params["n_mol"], box_ang=params["box_ang"],
                        periodic=params["periodic"], n_img_1d=params["n_img_1d"],
                        basis=params["basis"], n_occ=params["n_occ"], rc_ang=rc_ang,
                        eps_schwarz=eps_schwarz, seed=seed, full_enum=int(full_enum),
-                       max_prm=max_prm, max_ncontr=max_ncontr)
+                       max_prm=max_prm, max_ncontr=max_ncontr, setq_stride=setq_stride,
+                       setq_phase=setq_phase, threads=threads)
         self.name = name
         self.params = params
         self._w = driver().gd_create(ctypes.byref(cfg))
+        if not self._w:
+            raise RuntimeError("workload generation failed (too large for the 32-bit trace: sample it with setq_stride)")
         inf = GdInfo()
         driver().gd_get_info(self._w, ctypes.byref(inf))
         self.info = {f: getattr(inf, f) for f, _ in GdInfo._fields_}
@@ -221,10 +228,15 @@ class Session:
 class MultiSession:
     """nthreads handles of one library, driven by nthreads host threads (one handle per thread,
     as a caller with one handle per OpenMP thread uses the C-ABI); each thread streams a
-    contiguous share of the set quartets and the threads' K are summed."""
+    contiguous share of the set quartets.
 
-    def __init__(self, api, wl, nthreads, max_mem_mb=1000):
-        self.api, self.wl, self.n = api, wl, int(nthreads)
+    team=False: independent threads, each with its own K array; the threads' K are summed.
+    team=True:  the threads form one OpenMP team and pass one shared K array, as CP2K does; the
+                library's collective set_P/get_K leave the whole K in it (libraries without
+                team-collective calls, such as the oracle, cannot be driven this way)."""
+
+    def __init__(self, api, wl, nthreads, max_mem_mb=1000, team=False):
+        self.api, self.wl, self.n, self.team = api, wl, int(nthreads), bool(team)
         self.hs = [driver().gd_setup(wl._w, api._a, max_mem_mb) for _ in range(self.n)]
 
     def build_K(self, P=None, idx=None):
@@ -247,8 +259,11 @@ class MultiSession:
             driver().gd_mt_split(self.wl._w, ip, n, self.n, self._cut.ctypes.data_as(ctypes.POINTER(ctypes.c_long)))
             self._cut_key = key
             self._idx = idx
-        ms = driver().gd_build_K_mt(self.wl._w, self.api._a, arr, self.n, Pp, _dp(K), ip,
-                                    self._cut.ctypes.data_as(ctypes.POINTER(ctypes.c_long)), _dp(t))
+        fn = driver().gd_build_K_team if self.team else driver().gd_build_K_mt
+        ms = fn(self.wl._w, self.api._a, arr, self.n, Pp, _dp(K), ip,
+                self._cut.ctypes.data_as(ctypes.POINTER(ctypes.c_long)), _dp(t))
+        if ms < 0:
+            raise RuntimeError(f"the OpenMP team did not get {self.n} threads")
         return K, ms, t
 
     def close(self):

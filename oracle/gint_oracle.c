@@ -116,6 +116,18 @@ typedef struct {
    double ftable[121*28];
    int nthreads;
    int error;
+   /* optional screening-decision counters per class (the engine's libgint_get_counters layout):
+      [cls*4 + 0] Chebyshev evaluations, 1 Boys evaluations, 2 images through the VRR
+      (Fm[0] > 1e-12, classes other than (ss|ss)), 3 primitive quartets */
+   int counting;
+   unsigned long long cnt[256*4];
+   /* magnitude mode: every factor of every product replaced by its absolute value (the Chebyshev
+      coefficients and polynomials of G_m, the VRR factors, the contraction coefficients, AB/CD,
+      c2s, -fac and P), so that K holds, per element, the sum of the magnitudes of the terms its
+      FP64 evaluation adds up: the scale of the rounding error any evaluation order makes, against
+      which two FP64 implementations are compared. (The geometric factors themselves, P, Q, W and
+      their differences, are evaluated with the same rounded operations on both sides.) */
+   int absmode;
 } or_handle;
 
 /* ------------------------------------------------------------------------------------ */
@@ -231,7 +243,8 @@ static void or_fill_lut(or_handle *h) {
    }
 }
 
-/* returns 1 if the Boys function must be used instead (then res is zeroed) */
+/* returns 1 if the Boys function must be used instead (then res is zeroed), 2 when the Chebyshev
+   series was evaluated, 0 beyond the truncation (res zeroed) */
 static int or_tcg(const or_handle *h, double *res, double R, double T, int Nder, double Kfac) {
    double upper = R*R + 11.0*R + 50.0;
    double lower = R*R - 11.0*R + 0.0;
@@ -278,17 +291,24 @@ static int or_tcg(const or_handle *h, double *res, double R, double T, int Nder,
       T1[i] = 2.*TG1*T1[i-1] - T1[i-2];
       T2[i] = 2.*TG2*T2[i-1] - T2[i-2];
    }
+   if (h->absmode) {
+      /* magnitude of the series: the scale of its rounding error, not of its value */
+      for (int i = 0; i < 14; i++) { T1[i] = fabs(T1[i]); T2[i] = fabs(T2[i]); }
+   }
    for (int k = 0; k <= Nder; k++) {
       double tmp = 0.0;
       int jl = 0;
       for (int j = 0; j < 14; j++) {
          double dot = 0.0;
-         for (int l = 0; l < 14-j; l++) { dot += T1[l] * C0_row[k*105+jl]; jl++; }
+         for (int l = 0; l < 14-j; l++) {
+            const double cf = h->absmode ? fabs(C0_row[k*105+jl]) : C0_row[k*105+jl];
+            dot += T1[l] * cf; jl++;
+         }
          tmp += dot * T2[j];
       }
       res[k] = tmp*Kfac;
    }
-   return 0;
+   return 2;
 }
 
 /* ------------------------------------------------------------------------------------ */
@@ -533,7 +553,7 @@ static void or_hrr(const or_cls *c, const double *tin, const double AB[3], const
 }
 
 /* cart -> spherical, one centre at a time: a, then b, c, d (src/compute_SPH.cpp:127-234) */
-static void or_sph(int la, int lb, int lc, int ld, const double *cart, double *sph, double *ws) {
+static void or_sph(int la, int lb, int lc, int ld, const double *cart, double *sph, double *ws, int absmode) {
    int n[4] = {ncart(la), ncart(lb), ncart(lc), ncart(ld)};
    int s[4] = {nsph(la), nsph(lb), nsph(lc), nsph(ld)};
    int l[4] = {la, lb, lc, ld};
@@ -552,7 +572,8 @@ static void or_sph(int la, int lb, int lc, int ld, const double *cart, double *s
          for (int k = 0; k < n[ctr]; k++) {
             int jd[4] = {id[0], id[1], id[2], id[3]}; jd[ctr] = k;
             int si = ((jd[0]*dims[1] + jd[1])*dims[2] + jd[2])*dims[3] + jd[3];
-            acc += or_c2s[l[ctr]][id[ctr]][k] * src[si];
+            const double cf = or_c2s[l[ctr]][id[ctr]][k];
+            acc += (absmode ? fabs(cf) : cf) * src[si];
          }
          dst[t] = acc;
       }
@@ -566,7 +587,8 @@ static const double or_symm_factors[5] = {2.0, 1.0, 0.5, 0.25, 0.0};
 /* ------------------------------------------------------------------------------------ */
 /* one group: all image pairs of one set quartet for one l-combination                  */
 /* ------------------------------------------------------------------------------------ */
-static void or_group_compute(or_handle *h, const or_group *g, double *Kout[2], double *scratch) {
+static void or_group_compute(or_handle *h, const or_group *g, double *Kout[2], double *scratch,
+                             unsigned long long *cnt) {
    const int la = g->cls >> 6, lb = (g->cls >> 4) & 3, lc = (g->cls >> 2) & 3, ld = g->cls & 3;
    or_cls c; or_cls_init(&c, la, lb, lc, ld);
    const int L = c.L;
@@ -600,6 +622,7 @@ static void or_group_compute(or_handle *h, const or_group *g, double *Kout[2], d
       or_pbc(sc->R, sd->R, h->cell, CDs);
       for (int q = 0; q < 3; q++) { C[q] = sc->R[q]; D[q] = sc->R[q] + CDs[q] + h->neighs[n2*3+q]; }
 
+      cnt[g->cls*4 + 3] += (unsigned long long)sh->nprm;
       for (int ip = 0; ip < sh->nprm; ip++) {
          uint32_t code = h->prms.d[sh->prm_off + ip];
          int ipa = code >> 24, ipb = (code >> 16) & 255, ipc = (code >> 8) & 255, ipd = code & 255;
@@ -643,17 +666,23 @@ static void or_group_compute(or_handle *h, const or_group *g, double *Kout[2], d
             double PQ[3] = {P[0]-Q[0]-g3[0], P[1]-Q[1]-g3[1], P[2]-Q[2]-g3[2]};
             double rpq2 = (PQ[0]*PQ[0] + PQ[1]*PQ[1] + PQ[2]*PQ[2]);
             double T = rho * rpq2;
-            int use_gamma = or_tcg(h, Fm, R, T, L, Kfac);
-            if (use_gamma) or_fgamma0(L, T, Fm, h->ftable, Kfac);
+            const int branch = or_tcg(h, Fm, R, T, L, Kfac);
+            if (branch == 1) or_fgamma0(L, T, Fm, h->ftable, Kfac);
+            cnt[g->cls*4 + 0] += (branch == 2);
+            cnt[g->cls*4 + 1] += (branch == 1);
+            const int survives = Fm[0] > 1.e-12;
+            if (h->absmode) for (int m = 0; m <= L; m++) Fm[m] = fabs(Fm[m]);
             /* the (00|00) value enters the s-type target unscreened
                (src/compute_VRR.cpp:381-389 writes Fm[0] for every visited primitive) */
             if (want00) ssum[c.toff[0][0]] += Fm[0];
-            if (!(Fm[0] > 1.e-12)) continue;          /* src/compute_VRR.cpp:387 */
+            if (!survives) continue;                  /* Fm[0] > 1e-12, src/compute_VRR.cpp:387 */
+            cnt[g->cls*4 + 2] += (g->cls != 0);
             double Qp[3] = {Q[0]+g3[0], Q[1]+g3[1], Q[2]+g3[2]};
             double W[3]; wdist(W, P, Qp, zab, zcd2, invz);
             double pqz[17] = { PA[0], PA[1], PA[2], W[0]-P[0], W[1]-P[1], W[2]-P[2],
                                QC[0], QC[1], QC[2], W[0]-Qp[0], W[1]-Qp[1], W[2]-Qp[2],
                                i2ab, mrab, i2cd, mrcd, i2z };
+            if (h->absmode) for (int q = 0; q < 17; q++) pqz[q] = fabs(pqz[q]);
             or_vrr(&c, V, Fm, pqz);
             for (int e = la; e <= c.LAB; e++) for (int f = lc; f <= c.LCD; f++) {
                if (e == 0 && f == 0) continue;      /* added above, unscreened */
@@ -670,6 +699,7 @@ static void or_group_compute(or_handle *h, const or_group *g, double *Kout[2], d
             int cc = (l / g->nl[3]) % g->nl[2];
             int d = l % g->nl[3];
             double Kp = Ka[a*sa->np + ipa] * Kb[b*sb->np + ipb] * Kc[cc*sc->np + ipc] * Kd[d*sd->np + ipd];
+            if (h->absmode) Kp = fabs(Kp);
             double *dst = contr + (size_t)l*c.tsize;
             for (int q = 0; q < c.tsize; q++) dst[q] += Kp*ssum[q];
          }
@@ -677,6 +707,7 @@ static void or_group_compute(or_handle *h, const or_group *g, double *Kout[2], d
       /* HRR per contracted block + sum over (n1,n2) (src/compute_HRR.cpp:190-223) */
       double ABv[3] = {A[0]-B[0], A[1]-B[1], A[2]-B[2]};
       double CDv[3] = {C[0]-D[0], C[1]-D[1], C[2]-D[2]};
+      if (h->absmode) for (int q = 0; q < 3; q++) { ABv[q] = fabs(ABv[q]); CDv[q] = fabs(CDv[q]); }
       for (int l = 0; l < nlabcd; l++) {
          or_hrr(&c, contr + (size_t)l*c.tsize, ABv, CDv, cart, ws);
          double *dst = abcd0 + (size_t)l*Nc;
@@ -690,7 +721,7 @@ static void or_group_compute(or_handle *h, const or_group *g, double *Kout[2], d
    double *sph = cart;
    for (int r = 0; r < g->nqrtt && r < nlabcd; r++) {
       const or_qrtt *k = &h->qrtts.d[g->qrtt_off + r];
-      or_sph(la, lb, lc, ld, abcd0 + (size_t)r*Nc, sph, ws);
+      or_sph(la, lb, lc, ld, abcd0 + (size_t)r*Nc, sph, ws, h->absmode);
       const double fac = or_symm_factors[k->idx_fac] * h->hf_fac;
       for (int t = 0; t < Ns; t++) {
          const int isa = t / nsbcd, isb = (t / nscd) % nsb, isc = (t / nsd) % nsc, isd = t % nsd;
@@ -703,10 +734,17 @@ static void or_group_compute(or_handle *h, const or_group *g, double *Kout[2], d
          if (Iac >= h->FP_size || Iad >= h->FP_size || Ibc >= h->FP_size || Ibd >= h->FP_size) {
             h->error = 3; continue;
          }
-         const double iabcd = - fac * sph[t];
+         const double iabcd = h->absmode ? fabs(fac * sph[t]) : - fac * sph[t];
          for (int s = 0; s < h->nspin; s++) {
             const double *Pm = h->P[s];
             double *Km = Kout[s];
+            if (h->absmode) {
+               Km[Ibd] += iabcd * fabs(Pm[Iac]);
+               Km[Ibc] += iabcd * fabs(Pm[Iad]);
+               Km[Iad] += iabcd * fabs(Pm[Ibc]);
+               Km[Iac] += iabcd * fabs(Pm[Ibd]);
+               continue;
+            }
             Km[Ibd] += iabcd * Pm[Iac];
             Km[Ibc] += iabcd * Pm[Iad];
             Km[Iad] += iabcd * Pm[Ibc];
@@ -745,14 +783,20 @@ static void or_compute_all(or_handle *h) {
       tid = omp_get_thread_num();
 #endif
       double *scr = malloc(sizeof(double)*maxs);
+      unsigned long long *tcnt = calloc(256*4, sizeof(unsigned long long));
       double *Kloc[2] = {NULL, NULL};
       for (int s = 0; s < h->nspin; s++) {
          Kloc[s] = (tid == 0) ? h->K[s] : calloc(h->FP_size, sizeof(double));
          Kp[tid*2+s] = Kloc[s];
       }
       #pragma omp for schedule(dynamic, 4)
-      for (long ig = 0; ig < (long)h->groups.n; ig++) or_group_compute(h, &h->groups.d[ig], Kloc, scr);
+      for (long ig = 0; ig < (long)h->groups.n; ig++) or_group_compute(h, &h->groups.d[ig], Kloc, scr, tcnt);
       free(scr);
+      if (h->counting) {
+         #pragma omp critical
+         for (int q = 0; q < 256*4; q++) h->cnt[q] += tcnt[q];
+      }
+      free(tcnt);
    }
    for (int t = 1; t < nth; t++) for (int s = 0; s < h->nspin; s++) {
       double *src = Kp[t*2+s];
@@ -980,6 +1024,21 @@ int libgint_add_set_quartets(void *hh, int n, const int *sets, const int *shell_
    return ((or_handle*)hh)->error;
 }
 void oracle_set_threads(void *hh, int n) { ((or_handle*)hh)->nthreads = n; }
+/* magnitude mode (see or_handle.absmode): the following K builds accumulate sums of magnitudes */
+void oracle_set_absmode(void *hh, int on) { ((or_handle*)hh)->absmode = on != 0; }
+/* the screening-decision counters of the engine's extension (same layout as its
+   libgint_get_counters): on = 1 zeroes and starts them */
+void libgint_set_counters(void *hh, int on) {
+   or_handle *h = hh;
+   or_compute_all(h);
+   if (on) memset(h->cnt, 0, sizeof(h->cnt));
+   h->counting = on != 0;
+}
+void libgint_get_counters(void *hh, unsigned long long *out) {
+   or_handle *h = hh;
+   or_compute_all(h);
+   memcpy(out, h->cnt, sizeof(h->cnt));
+}
 void oracle_destroy(void *hh) {
    or_handle *h = hh;
    for (int i = 0; i < h->nsets; i++) for (int q = 0; q < h->sets[i].nL; q++) free(h->sets[i].K[q]);
@@ -1016,7 +1075,7 @@ int oracle_tcg(double R_cut_unused, const double *C0, int ld_C0, double R, doubl
    if (!init) { memset(&h, 0, sizeof(h)); or_fill_lut(&h); or_make_ftable(h.ftable); init = 1; }
    h.C0 = (double*)C0; h.ld_C0 = ld_C0;
    int g = or_tcg(&h, res, R, T, Nder, Kfac);
-   if (g) or_fgamma0(Nder, T, res, h.ftable, Kfac);
-   return g;
+   if (g == 1) or_fgamma0(Nder, T, res, h.ftable, Kfac);
+   return g == 1;
 }
 void oracle_pbc(const double *A, const double *B, const double *cell, double *AB) { or_pbc(A, B, cell, AB); }

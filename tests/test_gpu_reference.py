@@ -3,7 +3,7 @@
 oracle/_ref/libref_gint.so is the reference's own CUDA code (src/*.cpp), compiled unchanged for
 sm_100a by `make -C oracle ref` in the development container; it travels with the tree. Both
 libraries receive the identical add_* stream from the workload driver. The reference sums K with
-atomics in a nondeterministic order; the bound is 1e-11 * max|K| for l <= 3.
+atomics in a nondeterministic order; the bound is 1e-12 * max|K| for l <= 3.
 
 The reference's own K depends on its batch size (libgint_set_max_mem). For the l = 3 system
 below, multi-GB batches drift from run to run by ~3e-10 of max|K| (2.8e-10 and 3.3e-10 in two
@@ -21,6 +21,8 @@ import pytest
 
 from conftest import ORACLE_SO, REF_GINT_SO
 from libgint_b200.workload import Api, Session, Workload
+
+TOL = 1e-12
 
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not os.path.exists(REF_GINT_SO), reason="reference CUDA build absent")]
@@ -48,8 +50,8 @@ def test_small_l2_matches_reference_cuda(engine_so):
     print(f"small_l2: engine vs reference {rel_e:.3e}, oracle vs reference {rel_o:.3e}, "
           f"E_x ref {wl.exchange_energy(Kr):.12f} engine {wl.exchange_energy(Ke):.12f}; "
           f"reference {ms_r:.1f} ms engine {ms_e:.1f} ms")
-    assert rel_o <= 1e-11
-    assert rel_e <= 1e-11
+    assert rel_o <= TOL
+    assert rel_e <= TOL
 
 
 def test_periodic_small_matches_reference_cuda(engine_so):
@@ -59,7 +61,7 @@ def test_periodic_small_matches_reference_cuda(engine_so):
     scale = np.abs(Kr).max()
     rel = np.abs(Ke - Kr).max() / scale
     print(f"periodic 3 molecules: engine vs reference {rel:.3e}; reference {ms_r:.1f} ms engine {ms_e:.1f} ms")
-    assert rel <= 1e-11
+    assert rel <= TOL
 
 
 def test_periodic_l3_matches_reference_cuda(engine_so):
@@ -73,4 +75,4 @@ def test_periodic_l3_matches_reference_cuda(engine_so):
     dex = abs(wl.exchange_energy(Ke) - wl.exchange_energy(Kr))
     print(f"periodic l3 (f shells, general contractions): engine vs reference {rel:.3e}, |dEx| {dex:.3e}; "
           f"reference {ms_r:.1f} ms engine {ms_e:.1f} ms")
-    assert rel <= 1e-11
+    assert rel <= TOL

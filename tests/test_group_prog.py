@@ -44,7 +44,7 @@ def _run_generated(la, lb, lc, ld, T, AB, CD):
     lines = []
     for ln in body.splitlines():
         ln = ln.strip()
-        m = re.match(r"const double (\w+) = (.*);$", ln)
+        m = re.match(r"const (?:double|R) (\w+) = (.*);$", ln)
         if m:
             lines.append(f"{m.group(1)} = {m.group(2)}")
             continue
