@@ -103,6 +103,16 @@ int libgint_add_set_quartets(void *handle, int n, const int *sets, const int *sh
                              const unsigned int *qrtt_off, const unsigned char *qrtt_T);
 
 /* ---- extensions (no counterpart in the reference's C-ABI) ------------------------------- */
+/* No counterpart in the reference (its path is FP64 throughout). Mixed precision: shell quartets
+ * whose Schwarz bound sqrt((ab|ab)(cd|cd)) max|P| (given by libgint_add_shell_bound) is below thr
+ * run G_m, the VRR, the image sum, the contraction, the HRR and the spherical transform in FP32, for
+ * the classes with la+lb+lc+ld <= 3; the screening decisions, every other class and the K update
+ * stay FP64. thr <= 0 (the default) computes everything in FP64. Applies to the add_shell calls
+ * that follow. */
+void libgint_set_fp32_threshold(void *handle, double thr);
+/* No counterpart in the reference: the Schwarz bound of the shell quartet of the next
+ * libgint_add_shell (consumed by it; shells without one stay FP64). */
+void libgint_add_shell_bound(void *handle, double bound);
 /* last error code of the handle (0 = none); the text is returned by libgint_error_string */
 int libgint_last_error(void *handle);
 const char *libgint_error_string(void *handle);
@@ -156,8 +166,8 @@ int libgint_replay_noalloc(void *handle, const double *P_dev, double *K_dev, siz
  * evaluations, images through the VRR, primitive quartets; c = la*64 + lb*16 + lc*4 + ld */
 void libgint_set_counters(void *handle, int on);
 void libgint_get_counters(void *handle, unsigned long long *out);
-/* out[0..5] = shell quartets, primitive quartets, groups, batches, kernel launches, bytes
- * copied host -> device */
+/* out[0..7] = shell quartets, primitive quartets, groups, batches, kernel launches, bytes
+ * copied host -> device, shell quartets and primitive quartets computed in FP32 */
 void libgint_get_stats(void *handle, long long *out);
 /* the tables the engine builds on the host, for inspection and tests: Boys table [121*28],
  * c2s [4][70] (per l: rows m, columns cartesian), patch maps [2*128*128], per-patch (B,W) [207*4] */

@@ -58,6 +58,8 @@ SIGNATURES = {
     "libgint_get_stats": (None, [_V, ctypes.POINTER(ctypes.c_longlong)]),
     "libgint_fp64_peak_tflops": (ctypes.c_double, []),
     "libgint_host_tables": (None, [_D, _D, ctypes.POINTER(ctypes.c_ubyte), _D]),
+    "libgint_set_fp32_threshold": (None, [_V, ctypes.c_double]),
+    "libgint_add_shell_bound": (None, [_V, ctypes.c_double]),
 }
 
 

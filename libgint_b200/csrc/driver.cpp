@@ -170,6 +170,7 @@ struct SetQ {
 struct Shell {
    uint16_t n1, n2;
    uint32_t prm_begin, prm_end;
+   float bound;       // the screening estimate sqrt((ab|ab)(cd|cd)) max|P| of the shell quartet
 };
 
 }  // namespace
@@ -555,6 +556,7 @@ gd_workload *gd_create(const gd_config *cfg) {
          bool reach = d2 <= lim * lim;
          if (!reach) continue;
          Shell sh; sh.n1 = (uint16_t)pa.n1; sh.n2 = (uint16_t)pc.n1;
+         sh.bound = (float)(pa.Q * pc.Q * pmax);
          sh.prm_begin = (uint32_t)out.prims.size();
          for (int ia = 0; ia < da.np; ia++) for (int ib = 0; ib < db.np; ib++) {
             double qab = pa.q[(size_t)ia * db.np + ib];
@@ -696,6 +698,11 @@ long gd_get_shell_prims(const gd_workload *w, long h, uint32_t *out) {
    return (long)(sh.prm_end - sh.prm_begin);
 }
 
+// the screening estimate of every shell quartet, in the workload's shell order
+void gd_get_shell_bounds(const gd_workload *w, float *out) {
+   for (size_t h = 0; h < w->shells.size(); h++) out[h] = w->shells[h].bound;
+}
+
 // per set quartet {i,j,k,l,n_shells,n_prims} (for cost/class statistics)
 void gd_get_setq(const gd_workload *w, long *out) {
    for (size_t q = 0; q < w->setq.size(); q++) {
@@ -734,6 +741,8 @@ struct gd_api {
    fn_cell cell; fn_neighs neighs; fn_atom atom; fn_atomL atomL; fn_prm prm; fn_shell shell;
    fn_qrt qrt; fn_qrtt qrtt; fn_h addset; fn_h dispatch; fn_h destroy;
    fn_bulk bulk;   // libgint_add_set_quartets, if the library has it
+   fn_d fp32thr;   // libgint_set_fp32_threshold, if the library has it
+   fn_d bound;     // libgint_add_shell_bound, if the library has it
 };
 
 gd_api *gd_api_open(const char *path) {
@@ -762,6 +771,8 @@ gd_api *gd_api_open(const char *path) {
 #undef SYM
    a->destroy = (fn_h)dlsym(dl, "libgint_destroy_handle");
    a->bulk = (fn_bulk)dlsym(dl, "libgint_add_set_quartets");
+   a->fp32thr = (fn_d)dlsym(dl, "libgint_set_fp32_threshold");
+   a->bound = (fn_d)dlsym(dl, "libgint_add_shell_bound");
    return a;
 }
 
@@ -792,6 +803,11 @@ static double build_K_impl(const gd_workload *w, gd_api *a, void *h, const doubl
 static int g_reverse_prims = 0;
 static int g_bulk = 0;        // stream through libgint_add_set_quartets when the library has it
 void gd_set_bulk(int on) { g_bulk = on; }
+// mixed precision: every K build sets this threshold (libgint_set_fp32_threshold) and passes each
+// shell quartet's bound (libgint_add_shell_bound) before its add_shell, where the library has them;
+// 0 = FP64 (no bounds passed)
+static double g_fp32_thr = 0.0;
+void gd_set_fp32_threshold(double thr) { g_fp32_thr = thr; }
 static long g_only_shell = -1;   // replay only this shell (index within its set quartet), -1: all
 void gd_set_only_shell(long k) { g_only_shell = k; }
 // replay the primitive quartets of every shell in reverse order (a reordering of the same sums)
@@ -896,6 +912,8 @@ static double build_K_impl(const gd_workload *w, gd_api *a, void *h, const doubl
    const int S = (int)w->sets.size();
    if (!idx && (q1 < 0 || q1 > (long)w->setq.size())) q1 = (long)w->setq.size();
    auto t0 = clk::now();
+   if (a->fp32thr) a->fp32thr(h, g_fp32_thr);
+   const bool bounds = g_fp32_thr > 0.0 && a->bound;
    a->setP(h, const_cast<double *>(P ? P : w->Pflat.data()), (int)w->flat_size);
    auto t1 = clk::now();
    if (bulk && a->bulk) stream_bulk(w, a, h, q0, q1, idx);
@@ -911,6 +929,7 @@ static double build_K_impl(const gd_workload *w, gd_api *a, void *h, const doubl
             uint32_t c = w->prims[p];
             a->prm(h, c >> 24, (c >> 16) & 255, (c >> 8) & 255, c & 255);
          }
+         if (bounds) a->bound(h, (double)sh.bound);
          a->shell(h, q.i, q.j, q.k, q.l, sh.n1, sh.n2);
       }
       const int la = d4[0]->l, lb = d4[1]->l, lc = d4[2]->l, ld = d4[3]->l;

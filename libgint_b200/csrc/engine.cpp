@@ -276,20 +276,26 @@ struct Handle {
    std::vector<SetFast> fast;
    bool basis_dirty = true, ent_dirty = true;
    // device-resident data
-   DBuf d_pool, d_ents, d_neighs, d_C0, d_lut, d_bw, d_ft, d_plans, d_err, d_vops;
+   DBuf d_pool, d_ents, d_neighs, d_C0, d_C0f, d_lut, d_bw, d_ft, d_plans, d_err, d_vops;
    std::vector<VOp> vops;           // precompiled VRR instructions of all classes
    std::shared_ptr<Team> team;      // device P and K (shared by the handles of an OpenMP team)
    int nspin = 0;
    size_t FP_size = 0;
    ClassPlan plans[256];
+   // mixed precision: shell quartets whose Schwarz bound (libgint_add_shell_bound) is below the
+   // threshold run in FP32 where the class has an FP32 path; 0 = everything in FP64
+   double fp32_thr = 0.0;
+   double next_bound = HUGE_VAL;    // bound of the next add_shell (reset by it)
+   bool has_fp32[256];
    int S_of[256];                   // plans[c].S, kept compact for the streaming path
    bool plans_ready = false;
    // streaming state
    std::vector<uint32_t> prm_tmp;
    OpenGroup open[64];
    int nopen = 0;
-   int open_of[256];
-   ClassQ qs[2][256];               // queue sets, one per slot
+   // Queue classes: qc = c (FP64) or c + kFp32 (the same class in FP32), c = la*64+lb*16+lc*4+ld
+   int open_of[2 * 256];
+   ClassQ qs[2][2 * 256];           // queue sets, one per slot
    ClassQ *q = qs[0];               // the set being filled
    std::vector<int> active;
    size_t pend_prims = 0, pend_ac = 0, pend_rec = 0;
@@ -307,6 +313,7 @@ struct Handle {
    long long n_launch = 0;
    // statistics
    long long n_shells = 0, n_prims = 0, n_groups = 0, n_flush = 0, h2d_bytes = 0;
+   long long n_shells_fp32 = 0, n_prims_fp32 = 0;
 };
 
 static void set_error(Handle *h, int code, const std::string &msg) {
@@ -348,6 +355,15 @@ static bool in_team() {
 }
 
 static inline int cls_of(int la, int lb, int lc, int ld) { return la * 64 + lb * 16 + lc * 4 + ld; }
+
+constexpr int kFp32 = 256;          // queue-class offset of the FP32 variant of a class
+
+// queue class of the shell quartet being added: its class, in FP32 if its bound is below the
+// threshold and the class has an FP32 path (consumes the pending bound)
+static inline int shell_qclass(Handle *h, int c) {
+   const bool f32 = h->fp32_thr > 0.0 && h->next_bound < h->fp32_thr && h->has_fp32[c];
+   return f32 ? c + kFp32 : c;
+}
 
 static inline OpenGroup *open_group(Handle *h, int c) {
    int o = h->open_of[c];
@@ -447,6 +463,11 @@ static bool upload_tables(Handle *h) {
                         105 * sizeof(double));
       if (!ensure(h, h->d_C0, packed.size() * 8, "C0")) return false;
       if (!h2d(h, h->d_C0.p, packed.data(), packed.size() * 8, "C0")) return false;
+      // the FP32 path's copy, same layout
+      std::vector<float> packed_f(packed.begin(), packed.end());
+      if (!ensure(h, h->d_C0f, packed_f.size() * 4, "C0 (FP32)")) return false;
+      if (!h2d(h, h->d_C0f.p, packed_f.data(), packed_f.size() * 4, "C0 (FP32)")) return false;
+      if (!ck(h, cudaStreamSynchronize(h->stream), "C0 upload")) return false;
       h->pot_dirty = false;
       uploaded = true;
    }
@@ -506,6 +527,7 @@ static DevCtx make_ctx(Handle *h) {
    c.R_cut = h->R_cut;
    c.C0 = (const double *)h->d_C0.p;
    c.ld_C0 = (h->ld_C0 / 105) * kC0Row;
+   c.C0f = (const float *)h->d_C0f.p;
    c.lut_low = (const uint8_t *)h->d_lut.p;
    c.lut_high = (const uint8_t *)h->d_lut.p + 128 * 128;
    c.bw = (const double *)h->d_bw.p;
@@ -548,7 +570,7 @@ static void flush(Handle *h) {
    if (h->nspin == 0 || !h->team || !h->team->K[0].p) { set_error(h, 4, "work queued before libgint_set_P"); clear_queues(h); return; }
    if (!h->have_pot) { set_error(h, 4, "work queued before libgint_set_Potential_Truncated"); clear_queues(h); return; }
    for (int c : h->active) {
-      if (h->ld_C0 < (h->plans[c].L + 1) * 105) {
+      if (h->ld_C0 < (h->plans[c & 255].L + 1) * 105) {
          set_error(h, 2, "C0 holds fewer derivative orders than la+lb+lc+ld+1");
          clear_queues(h);
          return;
@@ -584,7 +606,7 @@ static void flush(Handle *h) {
       g.o_q = off; off = al16(off + Q.qrtts.size() * sizeof(QrttRec));
       g.o_rg = off; off = al16(off + Q.rowgrp.size() * 4);
       g.ac_off = ac;
-      ac += ((size_t)Q.prm.size() * h->plans[c].S + 1) & ~(size_t)1;
+      ac += ((size_t)Q.prm.size() * h->plans[c & 255].S + 1) & ~(size_t)1;
       segs.push_back(g);
    }
    if (!ensure(h, s.rec, std::max(off, (size_t)(64u << 20)), "record buffer")) return;
@@ -618,12 +640,13 @@ static void flush(Handle *h) {
    int nseg = 0;
    for (const Seg &g : segs) {
       ClassQ &Q = h->q[g.c];
-      const ClassPlan &hp = h->plans[g.c];
+      const ClassPlan &hp = h->plans[g.c & 255];
       BatchArgs bt;
       std::memset(&bt, 0, sizeof(bt));
       char *base = dev_rec;
-      bt.cls = g.c;
-      bt.plan = (const ClassPlan *)h->d_plans.p + g.c;
+      bt.cls = g.c & 255;
+      bt.fp32 = g.c >= kFp32;
+      bt.plan = (const ClassPlan *)h->d_plans.p + (g.c & 255);
       bt.prm = (const uint32_t *)(base + g.o_prm);
       bt.prm_shell = (const uint32_t *)(base + g.o_ps);
       bt.shells = (const ShellRec *)(base + g.o_sh);
@@ -647,6 +670,7 @@ static void flush(Handle *h) {
       h->n_launch += 2;
       if (rb) rb->segs.push_back({g.c, g.o_prm, g.o_ps, g.o_sh, g.o_g, g.o_q, g.o_rg, g.ac_off, bt.nprm, bt.nshell, bt.ngroup, bt.nqrtt});
       h->n_prims += bt.nprm; h->n_shells += bt.nshell; h->n_groups += bt.ngroup;
+      if (bt.fp32) { h->n_prims_fp32 += bt.nprm; h->n_shells_fp32 += bt.nshell; }
    }
    join_workers(h);
    ck(h, cudaEventRecord(s.ev, h->stream), "event record");
@@ -659,7 +683,7 @@ static void flush(Handle *h) {
    h->q = h->qs[h->cur];
    Slot &o = h->slots[h->cur];
    if (o.copy_busy) { ck(h, cudaEventSynchronize(o.ev_copy), "queue wait"); o.copy_busy = false; }
-   for (int c = 0; c < 256; c++) {
+   for (int c = 0; c < 2 * 256; c++) {
       ClassQ &Q = h->q[c];
       if (Q.prm.size() || Q.shells.size() || Q.qrtts.size() || Q.groups.size()) {
          Q.prm.clear(); Q.prm_shell.clear(); Q.shells.clear(); Q.groups.clear(); Q.qrtts.clear(); Q.rowgrp.clear();
@@ -773,7 +797,7 @@ static double replay_impl(Handle *h, double *kt, double *kcls = nullptr) {
    size_t ac = 0, gs = 0;
    for (auto &rb : h->recs) {
       ac = std::max(ac, rb.ac_doubles);
-      for (auto &g : rb.segs) { int a, b; gs = std::max(gs, group_global_scratch(h->plans[g.c], &a, &b)); }
+      for (auto &g : rb.segs) { int a, b; gs = std::max(gs, group_global_scratch(h->plans[g.c & 255], &a, &b)); }
    }
    // Every batch numbers its AC rows from 0, and the worker streams run the segments of
    // consecutive batches at the same time, so batches alternate between two halves of the replay
@@ -811,8 +835,9 @@ static double replay_impl(Handle *h, double *kt, double *kcls = nullptr) {
       for (auto &g : rb.segs) {
          BatchArgs bt;
          std::memset(&bt, 0, sizeof(bt));
-         bt.cls = g.c;
-         bt.plan = (const ClassPlan *)h->d_plans.p + g.c;
+         bt.cls = g.c & 255;
+         bt.fp32 = g.c >= kFp32;
+         bt.plan = (const ClassPlan *)h->d_plans.p + (g.c & 255);
          bt.prm = (const uint32_t *)(base + g.o_prm);
          bt.prm_shell = (const uint32_t *)(base + g.o_ps);
          bt.shells = (const ShellRec *)(base + g.o_sh);
@@ -823,13 +848,14 @@ static double replay_impl(Handle *h, double *kt, double *kcls = nullptr) {
          bt.AC = ac_half + g.ac_off;
          bt.gscratch = (double *)h->rec_gscr.p;
          int a_, b_;
-         cudaStream_t st = spread ? worker_for(h, nseg++, group_global_scratch(h->plans[g.c], &a_, &b_) != 0)
+         const ClassPlan &hp = h->plans[g.c & 255];
+         cudaStream_t st = spread ? worker_for(h, nseg++, group_global_scratch(hp, &a_, &b_) != 0)
                                   : h->stream;
          kmark();
-         if (kt) kcl.push_back(g.c);
-         if (!ck(h, launch_prim(ctx, bt, h->plans[g.c], st), "k_prim launch")) break;
+         if (kt) kcl.push_back(g.c & 255);
+         if (!ck(h, launch_prim(ctx, bt, hp, st), "k_prim launch")) break;
          kmark();
-         if (!ck(h, launch_group(ctx, bt, h->plans[g.c], st), "k_group launch")) break;
+         if (!ck(h, launch_group(ctx, bt, hp, st), "k_group launch")) break;
          kmark();
          h->n_launch += 2;
       }
@@ -870,11 +896,12 @@ extern "C" {
 void *libgint_create_handle(void) {
    Handle *h = new Handle();
    h->prm_tmp.reserve(65536);
-   for (int c = 0; c < 256; c++) h->open_of[c] = -1;
+   for (int c = 0; c < 2 * 256; c++) h->open_of[c] = -1;
    for (int c = 0; c < 256; c++) {
       build_class_plan(c >> 6, (c >> 4) & 3, (c >> 2) & 3, c & 3, h->plans[c]);
       build_vops(h->plans[c], h->vops);
       h->S_of[c] = h->plans[c].S;
+      h->has_fp32[c] = class_has_fp32(c >> 6, (c >> 4) & 3, (c >> 2) & 3, c & 3);
    }
    return h;
 }
@@ -1007,6 +1034,8 @@ static void add_shell_general(Handle *h, const int idx[4], int n1, int n2);
 void libgint_add_shell(void *hh, int i, int j, int k, int l, int n1, int n2) {
    Handle *h = (Handle *)hh;
    const size_t np = h->prm_tmp.size();
+   const double bound = h->next_bound;
+   h->next_bound = HUGE_VAL;        // a bound applies to one add_shell
    if (np == 0) return;
    const int ns = (int)h->sets.size();
    if ((unsigned)i >= (unsigned)ns || (unsigned)j >= (unsigned)ns || (unsigned)k >= (unsigned)ns ||
@@ -1031,7 +1060,9 @@ void libgint_add_shell(void *hh, int i, int j, int k, int l, int n1, int n2) {
       return;
    }
    if (fa.nL == 1 && fb.nL == 1 && fc.nL == 1 && fd.nL == 1) {
-      const int cl = cls_of(fa.l0, fb.l0, fc.l0, fd.l0);
+      h->next_bound = bound;
+      const int cl = shell_qclass(h, cls_of(fa.l0, fb.l0, fc.l0, fd.l0));
+      h->next_bound = HUGE_VAL;
       OpenGroup *og = open_group(h, cl);
       if (!og) { set_error(h, 2, "libgint_add_shell: too many l-combinations in one set quartet"); h->prm_tmp.clear(); return; }
       ClassQ &Q = h->q[cl];
@@ -1049,7 +1080,9 @@ void libgint_add_shell(void *hh, int i, int j, int k, int l, int n1, int n2) {
       return;
    }
    const int idx[4] = {i, j, k, l};
+   h->next_bound = bound;
    add_shell_general(h, idx, n1, n2);
+   h->next_bound = HUGE_VAL;
 }
 
 static void add_shell_general(Handle *h, const int idx[4], int n1, int n2) {
@@ -1057,7 +1090,7 @@ static void add_shell_general(Handle *h, const int idx[4], int n1, int n2) {
    const uint32_t np = (uint32_t)h->prm_tmp.size();
    for (int a = 0; a < S4[0]->nL; a++) for (int b = 0; b < S4[1]->nL; b++)
    for (int c = 0; c < S4[2]->nL; c++) for (int d = 0; d < S4[3]->nL; d++) {
-      const int cl = cls_of(S4[0]->l[a], S4[1]->l[b], S4[2]->l[c], S4[3]->l[d]);
+      const int cl = shell_qclass(h, cls_of(S4[0]->l[a], S4[1]->l[b], S4[2]->l[c], S4[3]->l[d]));
       OpenGroup *og = open_group(h, cl);
       if (!og) { set_error(h, 2, "libgint_add_shell: too many l-combinations in one set quartet"); break; }
       ClassQ &Q = h->q[cl];
@@ -1085,11 +1118,17 @@ void libgint_add_qrt(void *hh, int la, int lb, int lc, int ld, int nla, int nlb,
       set_error(h, 2, "libgint_add_qrt: l <= 3 and 1 <= nl <= 4");
       return;
    }
-   OpenGroup *og = open_group(h, cls_of(la, lb, lc, ld));
+   // the class's FP64 group, and its FP32 group if FP32 shell quartets were added
+   const int c = cls_of(la, lb, lc, ld);
+   OpenGroup *og = open_group(h, c);
    if (!og) { set_error(h, 2, "libgint_add_qrt: too many l-combinations in one set quartet"); return; }
    if (og->have_qrt) { set_error(h, 2, "libgint_add_qrt: the same l-combination twice in one set quartet"); return; }
-   og->nl[0] = (uint8_t)nla; og->nl[1] = (uint8_t)nlb; og->nl[2] = (uint8_t)nlc; og->nl[3] = (uint8_t)nld;
-   og->have_qrt = true;
+   OpenGroup *o32 = h->open_of[c + kFp32] >= 0 ? &h->open[h->open_of[c + kFp32]] : nullptr;
+   for (OpenGroup *g : {og, o32}) {
+      if (!g) continue;
+      g->nl[0] = (uint8_t)nla; g->nl[1] = (uint8_t)nlb; g->nl[2] = (uint8_t)nlc; g->nl[3] = (uint8_t)nld;
+      g->have_qrt = true;
+   }
 }
 
 void libgint_add_qrtt(void *hh, double symm_fac, int la, int lb, int lc, int ld, int inla, int inlb, int inlc, int inld,
@@ -1114,6 +1153,7 @@ void libgint_add_qrtt(void *hh, double symm_fac, int la, int lb, int lc, int ld,
    const int cl = cls_of(la, lb, lc, ld);
    OpenGroup *og = open_group(h, cl);
    if (!og) { set_error(h, 2, "libgint_add_qrtt: too many l-combinations in one set quartet"); return; }
+   OpenGroup *o32 = h->open_of[cl + kFp32] >= 0 ? &h->open[h->open_of[cl + kFp32]] : nullptr;
    QrttRec r;
    r.off[0] = off_ac; r.off[1] = off_ad; r.off[2] = off_bc; r.off[3] = off_bd;
    r.ld[0] = (uint8_t)ld_ac; r.ld[1] = (uint8_t)ld_ad; r.ld[2] = (uint8_t)ld_bc; r.ld[3] = (uint8_t)ld_bd;
@@ -1122,6 +1162,7 @@ void libgint_add_qrtt(void *hh, double symm_fac, int la, int lb, int lc, int ld,
    r.pad[0] = r.pad[1] = 0;
    h->q[cl].qrtts.push_back(r);
    og->nq++;
+   if (o32) { h->q[cl + kFp32].qrtts.push_back(r); o32->nq++; }   // the FP32 group updates the same rows
 }
 
 void libgint_add_set(void *hh) {
@@ -1151,7 +1192,7 @@ void libgint_add_set(void *hh) {
       if (!Q.active) { Q.active = true; h->active.push_back(og.cls); }
       const size_t added = Q.prm.size() - og.prm_off;
       h->pend_prims += added;
-      h->pend_ac += added * (size_t)h->S_of[og.cls];
+      h->pend_ac += added * (size_t)h->S_of[og.cls & 255];
       h->pend_rec += added * 8 + nshell * sizeof(ShellRec) + sizeof(GroupRec) + nrows * sizeof(QrttRec);
    }
    h->nopen = 0;
@@ -1278,6 +1319,15 @@ int libgint_add_set_quartets(void *hh, int n, const int *sets, const int *shell_
 
 void libgint_dispatch(void *hh) { flush((Handle *)hh); }
 
+// Mixed precision (no counterpart in the reference): shell quartets whose Schwarz bound
+// sqrt((ab|ab)(cd|cd)) max|P| is below thr run G_m, VRR, contraction, HRR and the spherical
+// transform in FP32 (classes with la+lb+lc+ld <= 3; the others, the screening decisions and the K
+// update stay FP64). thr <= 0 turns it off (the default). Applies to the add_shell calls that follow.
+void libgint_set_fp32_threshold(void *hh, double thr) { ((Handle *)hh)->fp32_thr = thr > 0.0 ? thr : 0.0; }
+
+// The Schwarz bound of the next add_shell's shell quartet (used by the mixed-precision threshold).
+void libgint_add_shell_bound(void *hh, double bound) { ((Handle *)hh)->next_bound = bound; }
+
 int libgint_last_error(void *hh) { return ((Handle *)hh)->err; }
 
 // The tables the engine builds on the host (for tests): Boys table (121*28), c2s for l<=3
@@ -1346,7 +1396,7 @@ int libgint_replay_noalloc(void *hh, const double *P_dev, double *K_dev, size_t 
    // every class segment must fit: image-summed targets [nprm][S], then the HRR workspace
    for (auto &rb : h->recs) {
       for (auto &g : rb.segs) {
-         const ClassPlan &hp = h->plans[g.c];
+         const ClassPlan &hp = h->plans[g.c & 255];
          int a = 0, b = 0;
          const size_t ac = ((size_t)g.nprm * hp.S + 31) & ~(size_t)31;
          const size_t need = ac + group_global_scratch(hp, &a, &b);
@@ -1354,7 +1404,7 @@ int libgint_replay_noalloc(void *hh, const double *P_dev, double *K_dev, size_t 
             char msg[256];
             std::snprintf(msg, sizeof(msg), "libgint_replay_noalloc: a recorded batch of class (%d%d|%d%d) needs %zu "
                           "doubles of scratch, the maximum is %zu; record with a smaller libgint_set_max_mem",
-                          g.c >> 6, (g.c >> 4) & 3, (g.c >> 2) & 3, g.c & 3, need, kNoAllocScratchDoubles);
+                          (g.c >> 6) & 3, (g.c >> 4) & 3, (g.c >> 2) & 3, g.c & 3, need, kNoAllocScratchDoubles);
             set_error(h, 5, msg);
             return h->err;
          }
@@ -1377,11 +1427,12 @@ int libgint_replay_noalloc(void *hh, const double *P_dev, double *K_dev, size_t 
    for (auto &rb : h->recs) {
       char *base = (char *)rb.rec.p;
       for (auto &g : rb.segs) {
-         const ClassPlan &hp = h->plans[g.c];
+         const ClassPlan &hp = h->plans[g.c & 255];
          BatchArgs bt;
          std::memset(&bt, 0, sizeof(bt));
-         bt.cls = g.c;
-         bt.plan = (const ClassPlan *)h->d_plans.p + g.c;
+         bt.cls = g.c & 255;
+         bt.fp32 = g.c >= kFp32;
+         bt.plan = (const ClassPlan *)h->d_plans.p + (g.c & 255);
          bt.prm = (const uint32_t *)(base + g.o_prm);
          bt.prm_shell = (const uint32_t *)(base + g.o_ps);
          bt.shells = (const ShellRec *)(base + g.o_sh);
@@ -1427,7 +1478,7 @@ void libgint_get_counters(void *hh, unsigned long long *out) {
 void libgint_get_stats(void *hh, long long *out) {
    Handle *h = (Handle *)hh;
    out[0] = h->n_shells; out[1] = h->n_prims; out[2] = h->n_groups; out[3] = h->n_flush; out[4] = h->n_launch;
-   out[5] = h->h2d_bytes;
+   out[5] = h->h2d_bytes; out[6] = h->n_shells_fp32; out[7] = h->n_prims_fp32;
 }
 
 double libgint_fp64_peak_tflops(void) { return measure_fp64_peak_tflops(); }
@@ -1541,7 +1592,7 @@ void libgint_destroy_handle(void *hh) {
    }
    for (auto &rb : h->recs) release(rb.rec);
    release(h->rec_ac); release(h->rec_gscr); release(h->d_cnt);
-   DBuf *bufs[] = {&h->d_pool, &h->d_ents, &h->d_neighs, &h->d_C0, &h->d_lut, &h->d_bw, &h->d_ft, &h->d_vops,
+   DBuf *bufs[] = {&h->d_pool, &h->d_ents, &h->d_neighs, &h->d_C0, &h->d_C0f, &h->d_lut, &h->d_bw, &h->d_ft, &h->d_vops,
                    &h->d_plans, &h->d_err};
    for (DBuf *b : bufs) release(*b);
    h->team.reset();

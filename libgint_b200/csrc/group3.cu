@@ -40,7 +40,9 @@ struct Group3Shape {
    static constexpr int MINB = L <= 1 ? 8 : (L == 2 ? 6 : 4);
 };
 
-template <int LA, int LB, int LC, int LD>
+// R = double: the FP64 path; R = float: the FP32 path (contraction, HRR and spherical transform in
+// FP32 from the FP32 targets of k_prim3; the K update in FP64).
+template <int LA, int LB, int LC, int LD, class R>
 __global__ void __launch_bounds__(128, Group3Shape<LA, LB, LC, LD>::MINB) k_group3(DevCtx ctx, BatchArgs bt) {
    using G = GrpGen<LA, LB, LC, LD>;
    constexpr int S = G::S, Nc = G::Nc, Ns = G::Ns;
@@ -58,9 +60,9 @@ __global__ void __launch_bounds__(128, Group3Shape<LA, LB, LC, LD>::MINB) k_grou
       const int nl1 = Gr.nl[1], nl2 = Gr.nl[2], nl3 = Gr.nl[3];
       const int r = (int)(q - Gr.qrtt_off);
       const int ia = r / (nl1 * nl2 * nl3), ib = (r / (nl2 * nl3)) % nl1, ic = (r / nl3) % nl2, id = r % nl3;
-      double cart[Nc];
+      R cart[Nc];
 #pragma unroll
-      for (int t = 0; t < Nc; t++) cart[t] = 0.0;
+      for (int t = 0; t < Nc; t++) cart[t] = R(0);
       for (uint32_t s = 0; s < Gr.nshell; s++) {
          const ShellRec sh = bt.shells[Gr.shell_off + s];
          const BasisEnt ea = ctx.ents[sh.ent[0]], eb = ctx.ents[sh.ent[1]];
@@ -69,27 +71,28 @@ __global__ void __launch_bounds__(128, Group3Shape<LA, LB, LC, LD>::MINB) k_grou
          const double *Kb = ctx.pool + eb.k_off + ib * eb.np;
          const double *Kc = ctx.pool + ec.k_off + ic * ec.np;
          const double *Kd = ctx.pool + ed.k_off + id * ed.np;
-         double T[S];
+         R T[S];
 #pragma unroll
-         for (int j = 0; j < S; j++) T[j] = 0.0;
+         for (int j = 0; j < S; j++) T[j] = R(0);
+         const R *AC = reinterpret_cast<const R *>(bt.AC);
          // contraction over the primitives (reference src/compute_ECO.cpp:131-212); two per
          // iteration so that the next one's loads overlap this one's FMAs
 #pragma unroll 2
          for (uint32_t ip = 0; ip < sh.nprm; ip++) {
             const uint32_t code = __ldg(bt.prm + sh.prm_off + ip);
-            const double kp = __ldg(Ka + (code >> 24)) * __ldg(Kb + ((code >> 16) & 255)) *
-                              __ldg(Kc + ((code >> 8) & 255)) * __ldg(Kd + (code & 255));
-            const double *row = bt.AC + (size_t)(sh.prm_off + ip) * S;
+            const R kp = (R)__ldg(Ka + (code >> 24)) * (R)__ldg(Kb + ((code >> 16) & 255)) *
+                         (R)__ldg(Kc + ((code >> 8) & 255)) * (R)__ldg(Kd + (code & 255));
+            const R *row = AC + (size_t)(sh.prm_off + ip) * S;
 #pragma unroll
             for (int j = 0; j < S; j++) T[j] += kp * __ldg(row + j);
          }
          double A[3], B[3], C[3], D[3], CDs[3];
          shell_geom(ctx, ea, eb, ec, ed, sh.n1, sh.n2, A, B, C, D, CDs);
-         const double AB[3] = {A[0] - B[0], A[1] - B[1], A[2] - B[2]};
-         const double CD[3] = {C[0] - D[0], C[1] - D[1], C[2] - D[2]};
+         const R AB[3] = {(R)(A[0] - B[0]), (R)(A[1] - B[1]), (R)(A[2] - B[2])};
+         const R CD[3] = {(R)(C[0] - D[0]), (R)(C[1] - D[1]), (R)(C[2] - D[2])};
          G::hrr(T, AB, CD, cart);
       }
-      double sph[Ns];
+      R sph[Ns];
       G::sph(cart, sph);
       const QrttRec k = bt.qrtts[q];
       const double fac = symm_factor(k.idx_fac) * ctx.hf_fac;
@@ -106,7 +109,7 @@ __global__ void __launch_bounds__(128, Group3Shape<LA, LB, LC, LD>::MINB) k_grou
             atomicOr(ctx.err, 1);
             continue;
          }
-         const double iabcd = -fac * sph[t];
+         const double iabcd = -fac * (double)sph[t];
          for (int sp = 0; sp < ctx.nspin; sp++) {
             const double *Pm = ctx.P[sp];
             double *Km = ctx.K[sp];
@@ -123,7 +126,8 @@ template <int LA, int LB, int LC, int LD>
 cudaError_t launch_one(const DevCtx &ctx, const BatchArgs &bt, cudaStream_t st) {
    const int threads = 128;
    const long blocks = std::max(1L, std::min(((long)bt.nqrtt + threads - 1) / threads, 148L * 16));
-   k_group3<LA, LB, LC, LD><<<(unsigned)blocks, threads, 0, st>>>(ctx, bt);
+   if (bt.fp32) k_group3<LA, LB, LC, LD, float><<<(unsigned)blocks, threads, 0, st>>>(ctx, bt);
+   else k_group3<LA, LB, LC, LD, double><<<(unsigned)blocks, threads, 0, st>>>(ctx, bt);
    return cudaGetLastError();
 }
 
@@ -152,7 +156,9 @@ struct PartPreload {
       } else {
          constexpr int c = kGrpGenClasses[I];
          cudaFuncAttributes a;
-         cudaError_t e = cudaFuncGetAttributes(&a, k_group3<(c >> 6) & 3, (c >> 4) & 3, (c >> 2) & 3, c & 3>);
+         cudaError_t e = cudaFuncGetAttributes(&a, k_group3<(c >> 6) & 3, (c >> 4) & 3, (c >> 2) & 3, c & 3, double>);
+         if (e != cudaSuccess) return e;
+         e = cudaFuncGetAttributes(&a, k_group3<(c >> 6) & 3, (c >> 4) & 3, (c >> 2) & 3, c & 3, float>);
          if (e != cudaSuccess) return e;
          return PartPreload<I + kGroup3Parts>::run();
       }

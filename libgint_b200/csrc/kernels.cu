@@ -858,6 +858,7 @@ cudaError_t launch_prim(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan 
       cudaError_t err = cudaSuccess;
       if (prim3_launch(ctx, bt, st, &err)) return err;
    }
+   if (bt.fp32) return cudaErrorInvalidValue;   // FP32 segments exist only for classes with k_prim3
    {
       const bool lane = prim2_lane(hp);
       int cp = 1;
@@ -920,6 +921,7 @@ cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan
       cudaError_t err = cudaSuccess;
       if (group3_launch(ctx, bt, st, &err)) return err;
    }
+   if (bt.fp32) return cudaErrorInvalidValue;   // FP32 segments exist only for classes with k_group3
    const size_t wd = group_warp_doubles(hp);
    if (wd <= 40) {
       // small workspace: one lane per group, 32 groups per warp

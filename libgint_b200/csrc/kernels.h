@@ -23,6 +23,7 @@ struct DevCtx {
    double R_cut;
    const double *C0;          // the caller's Chebyshev table repacked: per patch, (nder+1) rows of
    int ld_C0;                 // kC0Row doubles (105 coefficients, 3 zeros); ld_C0 = patch stride
+   const float *C0f;          // the same table rounded to FP32, same layout (the FP32 path)
    const uint8_t *lut_low, *lut_high;   // 128 x 128 patch maps
    const double *bw;          // per patch: B1, W1, B2, W2
    const double *ftable;      // Boys table, 121 x 28
@@ -55,7 +56,8 @@ struct BatchArgs {
    uint32_t nprm, nshell, ngroup;
    uint32_t nqrtt;            // contraction rows (the group kernels' work items), in group order
    const uint32_t *rowgrp;    // group of row 32 k, k < (nqrtt + 31) / 32
-   double *AC;                // [nprm][S] image-summed VRR targets
+   double *AC;                // [nprm][S] image-summed VRR targets (floats in the first half for fp32)
+   int fp32;                  // 1: the segment's shell quartets run in FP32 (Fm, VRR, contraction, HRR)
    double *gscratch;          // HRR workspace in global memory for the largest classes
    int cls;                   // la*64 + lb*16 + lc*4 + ld
 };
@@ -68,6 +70,8 @@ cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan
 size_t group_global_scratch(const ClassPlan &hp, int *grid, int *warps);
 constexpr int kGroupKpDoubles = 32;   // per-warp shared buffer of contraction coefficients in k_group
 int prim_team_size(const ClassPlan &hp);
+// classes with an FP32 path (generated VRR and HRR code): la + lb + lc + ld <= 3
+constexpr bool class_has_fp32(int la, int lb, int lc, int ld) { return la + lb + lc + ld <= 3; }
 // Fixed device scratch (file-scope device array in kernels.cu) used by libgint_replay_noalloc:
 // its device address for the current device; the first call on a device looks it up.
 constexpr size_t kNoAllocScratchDoubles = (size_t)8 * 1024 * 1024;   // 64 MiB

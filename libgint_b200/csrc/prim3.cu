@@ -52,23 +52,25 @@ struct Prim3Shape {
 };
 
 // Segmented sum over adjacent lanes that carry the same key (keys are contiguous runs); the
-// first lane of each run adds the run's sum to dst[s].
+// first lane of each run adds the run's sum to dst[s]. R = double, or float on the FP32 path.
+template <class R>
 struct SegSum {
    unsigned same;   // bit o: lane + 2^o carries this lane's key
    bool head;
-   double *dst;
-   __device__ __forceinline__ void operator()(int s, double v) {
+   R *dst;
+   __device__ __forceinline__ void operator()(int s, R v) {
 #pragma unroll
       for (int o = 0; o < 5; o++) {
-         const double u = __shfl_down_sync(kFull, v, 1 << o);
+         const R u = __shfl_down_sync(kFull, v, 1 << o);
          if (same & (1u << o)) v += u;
       }
       if (head) dst[s] += v;
    }
 };
 
-static __device__ __forceinline__ SegSum make_segsum(int key, int lane, double *dst) {
-   SegSum sg;
+template <class R>
+static __device__ __forceinline__ SegSum<R> make_segsum(int key, int lane, R *dst) {
+   SegSum<R> sg;
    sg.same = 0;
 #pragma unroll
    for (int o = 0; o < 5; o++) {
@@ -81,7 +83,9 @@ static __device__ __forceinline__ SegSum make_segsum(int key, int lane, double *
    return sg;
 }
 
-template <int LA, int LB, int LC, int LD>
+// R = double: the FP64 path; R = float: the FP32 path (G_m series, VRR, image sum and the stored
+// targets in FP32; the geometry and every screening decision in FP64 as on the FP64 path).
+template <int LA, int LB, int LC, int LD, class R>
 __global__ void __launch_bounds__(Prim3Shape<LA, LB, LC, LD>::THREADS, Prim3Shape<LA, LB, LC, LD>::MINB)
 k_prim3(DevCtx ctx, BatchArgs bt) {
    using Sh = Prim3Shape<LA, LB, LC, LD>;
@@ -98,11 +102,11 @@ k_prim3(DevCtx ctx, BatchArgs bt) {
    __syncthreads();
    double *wbase = smem + ((3 * Ng + 1) & ~1) + (size_t)warp * Sh::WD;
    PrimGeo *geo = reinterpret_cast<PrimGeo *>(wbase);
-   double *acc = wbase + CP * Sh::PG;
-   double *q1t = acc + CP * S;
+   R *acc = reinterpret_cast<R *>(wbase + CP * Sh::PG);
+   double *q1t = wbase + CP * Sh::PG + CP * S;
    int *q1i = reinterpret_cast<int *>(q1t + 64);
-   double *q2f = q1t + 64 + 32;
-   int *q2i = reinterpret_cast<int *>(q2f + 64 * LF);
+   R *q2f = reinterpret_cast<R *>(q1t + 64 + 32);
+   int *q2i = reinterpret_cast<int *>(q1t + 64 + 32 + 64 * LF);
    // pair numbering within a chunk: pair = p * Ng + n3; each round of 32 pairs advances a lane
    // by 32 = adv_p * Ng + adv_n
    const int adv_p = 32 / Ng, adv_n = 32 - adv_p * Ng;
@@ -118,7 +122,7 @@ k_prim3(DevCtx ctx, BatchArgs bt) {
          prim_geometry(ctx, bt.shells[bt.prm_shell[p0 + lane]], bt.prm[p0 + lane], g);
          geo[lane] = g;
       }
-      for (int j = lane; j < CP * S; j += 32) acc[j] = 0.0;
+      for (int j = lane; j < CP * S; j += 32) acc[j] = R(0);
       __syncwarp();
 
       int n1 = 0, n2 = 0;
@@ -128,20 +132,20 @@ k_prim3(DevCtx ctx, BatchArgs bt) {
          const int pk = act ? q2i[lane] : 0;
          const int p = pk >> 8, n3 = pk & 255;
          const PrimGeo &g = geo[p];
-         double z[17], F[LF];
+         R z[17], F[LF];
 #pragma unroll
          for (int q = 0; q < 3; q++) {
             const double Qp = g.Q[q] + sneigh[n3 * 3 + q];
             const double W = wdist(g.zab, g.P[q], g.zcd, Qp, g.inv_z);
-            z[q] = g.PA[q];
-            z[3 + q] = W - g.P[q];
-            z[6 + q] = g.QC[q];
-            z[9 + q] = W - Qp;
+            z[q] = (R)g.PA[q];
+            z[3 + q] = (R)(W - g.P[q]);
+            z[6 + q] = (R)g.QC[q];
+            z[9 + q] = (R)(W - Qp);
          }
-         z[12] = g.i2ab; z[13] = g.mrab; z[14] = g.i2cd; z[15] = g.mrcd; z[16] = g.i2z;
+         z[12] = (R)g.i2ab; z[13] = (R)g.mrab; z[14] = (R)g.i2cd; z[15] = (R)g.mrcd; z[16] = (R)g.i2z;
 #pragma unroll
-         for (int m = 0; m < LF; m++) F[m] = act ? q2f[lane * LF + m] : 0.0;
-         SegSum sg = make_segsum(act ? p : -1 - lane, lane, acc + p * S);
+         for (int m = 0; m < LF; m++) F[m] = act ? q2f[lane * LF + m] : R(0);
+         SegSum<R> sg = make_segsum<R>(act ? p : -1 - lane, lane, acc + p * S);
          G::run(F, z, sg);
          c_vrr += (lane == 0) ? (unsigned)cnt : 0u;
          __syncwarp();
@@ -151,19 +155,21 @@ k_prim3(DevCtx ctx, BatchArgs bt) {
          const bool act = lane < cnt;
          const int pk = act ? q1i[lane] : 0;
          const int p = pk >> 8;
-         double fm[LF];
+         R fm[LF];
          bool surv = false;
          if (act) {
-            const int br = fm_eval_geo<L>(ctx, L, geo[p], q1t[lane], fm);
+            int br;
+            if constexpr (sizeof(R) == sizeof(double)) br = fm_eval_geo<L>(ctx, L, geo[p], q1t[lane], fm);
+            else br = fm_eval_geo_f<L>(ctx, L, geo[p], q1t[lane], fm);
             c_cheb += (br == 1);
             c_boys += (br == 2);
-            surv = NEED_VRR && (fm[0] > 1.e-12);
+            surv = NEED_VRR && (fm[0] > R(1.e-12));
          } else {
 #pragma unroll
-            for (int m = 0; m < LF; m++) fm[m] = 0.0;
+            for (int m = 0; m < LF; m++) fm[m] = R(0);
          }
          if (W00) {
-            SegSum sg = make_segsum(act ? p : -1 - lane, lane, acc + p * S);
+            SegSum<R> sg = make_segsum<R>(act ? p : -1 - lane, lane, acc + p * S);
             sg(G::s00, fm[0]);
             __syncwarp();
          }
@@ -181,7 +187,7 @@ k_prim3(DevCtx ctx, BatchArgs bt) {
                run_vrr(32);
                const int rem = n2 - 32;
                int v = 0;
-               double tmp[LF];
+               R tmp[LF];
                if (lane < rem) {
                   v = q2i[32 + lane];
 #pragma unroll
@@ -239,7 +245,7 @@ k_prim3(DevCtx ctx, BatchArgs bt) {
       if (NEED_VRR && n2 > 0) run_vrr(n2);
       __syncwarp();
       if (lane == 0 && ctx.cnt) atomicAdd(ctx.cnt + bt.cls * 4 + 3, (unsigned long long)np);
-      double *out = bt.AC + (size_t)p0 * S;
+      R *out = reinterpret_cast<R *>(bt.AC) + (size_t)p0 * S;
       for (int j = lane; j < np * S; j += 32) out[j] = acc[j];
       __syncwarp();
    }
@@ -257,7 +263,7 @@ k_prim3(DevCtx ctx, BatchArgs bt) {
    }
 }
 
-template <int LA, int LB, int LC, int LD>
+template <int LA, int LB, int LC, int LD, class R>
 cudaError_t launch_one(const DevCtx &ctx, const BatchArgs &bt, cudaStream_t st) {
    using Sh = Prim3Shape<LA, LB, LC, LD>;
    const size_t warp_bytes = (size_t)Sh::WD * 8;
@@ -269,7 +275,7 @@ cudaError_t launch_one(const DevCtx &ctx, const BatchArgs &bt, cudaStream_t st) 
    const size_t smem = neigh_bytes + warp_bytes * nw;
    const long nchunk = ((long)bt.nprm + Sh::CP - 1) / Sh::CP;
    const long blocks = std::max(1L, std::min((nchunk + nw - 1) / nw, 148L * 24));
-   k_prim3<LA, LB, LC, LD><<<(unsigned)blocks, nw * 32, smem, st>>>(ctx, bt);
+   k_prim3<LA, LB, LC, LD, R><<<(unsigned)blocks, nw * 32, smem, st>>>(ctx, bt);
    return cudaGetLastError();
 }
 
@@ -281,7 +287,13 @@ struct PartTable {
       } else {
          constexpr int c = kVrrGenClasses[I];
          if (cls == c) {
-            *err = launch_one<(c >> 6) & 3, (c >> 4) & 3, (c >> 2) & 3, c & 3>(ctx, bt, st);
+            if (!bt.fp32) {
+               *err = launch_one<(c >> 6) & 3, (c >> 4) & 3, (c >> 2) & 3, c & 3, double>(ctx, bt, st);
+            } else if constexpr (class_has_fp32((c >> 6) & 3, (c >> 4) & 3, (c >> 2) & 3, c & 3)) {
+               *err = launch_one<(c >> 6) & 3, (c >> 4) & 3, (c >> 2) & 3, c & 3, float>(ctx, bt, st);
+            } else {
+               *err = cudaErrorInvalidValue;   // the engine queues FP32 work only for classes with a path
+            }
             return true;
          }
          return PartTable<I + kPrim3Parts>::launch(cls, ctx, bt, st, err);
@@ -297,9 +309,14 @@ struct PartPreload {
          return cudaSuccess;
       } else {
          constexpr int c = kVrrGenClasses[I];
-         cudaError_t e = cudaFuncSetAttribute(k_prim3<(c >> 6) & 3, (c >> 4) & 3, (c >> 2) & 3, c & 3>,
+         cudaError_t e = cudaFuncSetAttribute(k_prim3<(c >> 6) & 3, (c >> 4) & 3, (c >> 2) & 3, c & 3, double>,
                                               cudaFuncAttributeMaxDynamicSharedMemorySize, smax);
          if (e != cudaSuccess) return e;
+         if constexpr (class_has_fp32((c >> 6) & 3, (c >> 4) & 3, (c >> 2) & 3, c & 3)) {
+            e = cudaFuncSetAttribute(k_prim3<(c >> 6) & 3, (c >> 4) & 3, (c >> 2) & 3, c & 3, float>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smax);
+            if (e != cudaSuccess) return e;
+         }
          return PartPreload<I + kPrim3Parts>::run(smax);
       }
    }

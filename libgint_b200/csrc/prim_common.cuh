@@ -223,6 +223,51 @@ static __device__ __forceinline__ void cheb_eval(const DevCtx &ctx, int L_rt, in
    }
 }
 
+// four consecutive floats from a 16-byte aligned, read-only global address
+static __device__ __forceinline__ void ldg_v4f(const float *p, float *v) {
+   asm("ld.global.nc.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]) : "l"(p));
+}
+
+// cheb_eval in FP32 (the mixed-precision path): the patch and its mapped coordinates come from
+// the same FP64 decisions; the polynomials, the FP32 copy of the coefficients and the sums are FP32.
+template <int LT>
+static __device__ __forceinline__ void cheb_eval_f(const DevCtx &ctx, int L_rt, int patch, double X1, double X2,
+                                                   double Kfac, float *res) {
+   const int L = LT >= 0 ? LT : L_rt;
+   const double B1 = __ldg(ctx.bw + patch * 4 + 0), W1 = __ldg(ctx.bw + patch * 4 + 1);
+   const double B2 = __ldg(ctx.bw + patch * 4 + 2), W2 = __ldg(ctx.bw + patch * 4 + 3);
+   const float *C0_row = ctx.C0f + (size_t)ctx.ld_C0 * patch;
+   const float SQ2 = 1.41421356237309505f;
+   const float TG1 = (float)((2. * X1 - B1) * W1);
+   const float TG2 = (float)((2. * X2 - B2) * W2);
+   const float kf = (float)Kfac;
+   float T1[14], T2[14];
+   T1[0] = 1.0f; T2[0] = 1.0f;
+   T1[1] = SQ2 * TG1; T2[1] = SQ2 * TG2;
+   T1[2] = 2.f * TG1 * T1[1] - SQ2; T2[2] = 2.f * TG2 * T2[1] - SQ2;
+#pragma unroll
+   for (int i = 3; i < 14; i++) {
+      T1[i] = 2.f * TG1 * T1[i - 1] - T1[i - 2];
+      T2[i] = 2.f * TG2 * T2[i - 1] - T2[i - 2];
+   }
+   for (int k = 0; k <= L; k++) {
+      const float *c = C0_row + k * kC0Row;
+      float cf[kC0Row];
+#pragma unroll
+      for (int q = 0; q < kC0Row / 4; q++) ldg_v4f(c + 4 * q, cf + 4 * q);
+      float tmp = 0.0f;
+      int jl = 0;
+#pragma unroll
+      for (int j = 0; j < 14; j++) {
+         float dot = 0.0f;
+#pragma unroll
+         for (int l = 0; l < 14 - j; l++) { dot += T1[l] * cf[jl]; jl++; }
+         tmp += dot * T2[j];
+      }
+      res[k] = tmp * kf;
+   }
+}
+
 // ---------------------------------------------------------------------------------------
 // Truncated-Coulomb G_m(T,R) * Kfac (reference src/t_c_g0_n.cpp:67-180); falls back to the
 // Boys function for R > 11 and T < R^2 - 11 R.
@@ -324,6 +369,39 @@ static __device__ __forceinline__ uint32_t row_group_one(const BatchArgs &bt, ui
    const uint32_t gi = g0 + 1u + (uint32_t)lane;
    const bool later = gi < bt.ngroup && __ldg(&bt.groups[gi].qrtt_off) <= q;
    return g0 + __popc(__ballot_sync(0xffffffffu, later));
+}
+
+// fm_eval_geo for the FP32 path: the same decisions (truncation, branch, patch) in FP64, the
+// Chebyshev series in FP32 and the rarely taken Boys branch in FP64, rounded to FP32.
+template <int LT>
+static __device__ __forceinline__ int fm_eval_geo_f(const DevCtx &ctx, int L_rt, const PrimGeo &g, double T,
+                                                    float *res) {
+   const int L = LT >= 0 ? LT : L_rt;
+   if (T > g.upper) {
+      for (int n = 0; n <= L; n++) res[n] = 0.0f;
+      return 0;
+   }
+   double X1;
+   int patch;
+   if (g.lowR) {
+      X1 = rsub(T, 0.0) / rsub(g.upper, 0.0);
+      int i1 = (int)(X1 * 128);
+      if (i1 == 128) i1 = 127;
+      patch = __ldg(ctx.lut_low + i1 * 128 + g.i2);
+   } else {
+      if (T < g.lower) {
+         double tmp[kMaxLL + 1];
+         boys_eval_t<LT>(L, T, tmp, ctx.ftable, g.Kfac);
+         for (int n = 0; n <= L; n++) res[n] = (float)tmp[n];
+         return 2;
+      }
+      X1 = rsub(T, g.lower) / rsub(g.upper, g.lower);
+      int i1 = (int)(X1 * 128);
+      if (i1 == 128) i1 = 127;
+      patch = __ldg(ctx.lut_high + i1 * 128 + g.i2);
+   }
+   cheb_eval_f<LT>(ctx, L, patch, X1, g.X2, g.Kfac, res);
+   return 1;
 }
 
 }  // namespace gint

@@ -84,6 +84,10 @@ def driver():
         lib.gd_mt_split.restype = None
         lib.gd_mt_split.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_long), ctypes.c_long, ctypes.c_int,
                                     ctypes.POINTER(ctypes.c_long)]
+        lib.gd_set_fp32_threshold.restype = None
+        lib.gd_set_fp32_threshold.argtypes = [ctypes.c_double]
+        lib.gd_get_shell_bounds.restype = None
+        lib.gd_get_shell_bounds.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]
         lib.gd_set_bulk.restype = None
         lib.gd_set_bulk.argtypes = [ctypes.c_int]
         lib.gd_get_coeffs.restype = ctypes.c_int
@@ -169,6 +173,12 @@ class Workload:
         K = np.zeros(64); Z = np.zeros(16); nl = ctypes.c_int()
         np_ = driver().gd_get_coeffs(self._w, s, _dp(K), _dp(Z), ctypes.byref(nl))
         return K[:nl.value * np_].reshape(nl.value, np_), Z[:np_]
+
+    def shell_bounds(self):
+        """The screening estimate sqrt((ab|ab)(cd|cd)) max|P| of every shell quartet."""
+        out = np.empty(self.info["n_shells"], dtype=np.float32)
+        driver().gd_get_shell_bounds(self._w, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
+        return out
 
     def setq(self):
         out = np.empty((self.info["n_setq"], 6), dtype=np.int64)
@@ -271,6 +281,13 @@ class MultiSession:
             if h:
                 driver().gd_teardown(self.api._a, h)
         self.hs = []
+
+
+def set_fp32_threshold(thr):
+    """Mixed precision for the following K builds: every build sets this threshold in libraries
+    that export libgint_set_fp32_threshold and passes each shell quartet's screening bound
+    (libgint_add_shell_bound) before its add_shell; 0 turns it off (FP64)."""
+    driver().gd_set_fp32_threshold(float(thr))
 
 
 def set_bulk(on):
