@@ -20,8 +20,11 @@
  *   - libgint_destroy_handle releases a handle;
  *   - record/replay of the device-resident quartet list, counters and statistics are
  *     extensions declared at the end of this header.
- * Threading: one handle per host thread; handles are independent (each owns its stream and
- * device buffers), so the reference's team-collective calls need no omp barrier here.
+ * Threading: one handle per host thread (each owns its streams and queues). As in the reference,
+ * libgint_set_P, libgint_set_K and libgint_get_K (and their _polarized forms) are collective over
+ * the calling thread's OpenMP team: the team's handles share one device P and K, and get_K copies
+ * the team's whole K once (src/libGint.cpp:436-447, 555-628). Outside a parallel region a handle
+ * is a team of one.
  */
 #ifndef LIBGINT_B200_H
 #define LIBGINT_B200_H
@@ -136,7 +139,9 @@ int libgint_hrr_program(int la, int lb, int lc, int ld, unsigned int *out, int c
  * info_cap >= 4 + 5 ntg. Returns the instruction count (-1: unsupported class). No GPU needed. */
 int libgint_vrr_program(int la, int lb, int lc, int ld, void *vops, int cap, int *info, int info_cap);
 /* on = 1: keep the device batches of the following K build(s) (the screened quartet list of
- * an SCF step); on = 0: stop recording */
+ * an SCF step); on = 0: stop recording. libgint_replay captures the whole replay (every class
+ * segment's kernels on the worker streams) into a CUDA graph once and relaunches it while the
+ * recording, P/K buffers and kernel choices stay the same. */
 void libgint_record(void *handle, int on);
 /* recompute K from the recorded quartet list with the current P (after libgint_set_P), without
  * the add_* stream; K is then read with libgint_get_K. Returns the device time in ms. */
@@ -146,6 +151,16 @@ double libgint_replay(void *handle);
 double libgint_replay_profile(void *handle, double *kt);
 /* libgint_replay_profile plus the per-class split: kcls[c*2 + {0,1}] (ms), c as above */
 double libgint_replay_profile_classes(void *handle, double *kt, double *kcls);
+/* No counterpart in the reference. Per-class kernel choice: after libgint_record and libgint_set_P,
+ * libgint_autotune times, for every class of the recorded quartet list, the primitive kernel with
+ * generated per-lane VRR against the per-warp interpreted one, and the group kernel with one lane
+ * per contraction row (generated HRR) against one warp per row (interpreted HRR), and keeps the
+ * faster of each for every following launch; out[2c], out[2c+1] (c = la*64+lb*16+lc*4+ld; 512 ints,
+ * may be NULL) receive the choices (0 = per-lane, 1 = per-warp). libgint_set_tuning installs such a
+ * table, libgint_get_tuning reads it. Returns 0 or the error code. */
+int libgint_autotune(void *handle, int *out);
+void libgint_set_tuning(void *handle, const int *in);
+void libgint_get_tuning(void *handle, int *out);
 /* algorithmic FP64 operation counts of class (la,lb,lc,ld) following the reference recursion:
  * out[0] per Chebyshev G_m evaluation, [1] per Boys evaluation, [2] VRR per image, [3] image
  * sum per image, [4] contraction per primitive and row, [5] HRR per shell and row,

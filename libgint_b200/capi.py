@@ -59,6 +59,9 @@ SIGNATURES = {
     "libgint_fp64_peak_tflops": (ctypes.c_double, []),
     "libgint_host_tables": (None, [_D, _D, ctypes.POINTER(ctypes.c_ubyte), _D]),
     "libgint_set_fp32_threshold": (None, [_V, ctypes.c_double]),
+    "libgint_autotune": (ctypes.c_int, [_V, _I]),
+    "libgint_set_tuning": (None, [_V, _I]),
+    "libgint_get_tuning": (None, [_V, _I]),
     "libgint_add_shell_bound": (None, [_V, ctypes.c_double]),
 }
 

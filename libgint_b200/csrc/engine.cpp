@@ -287,6 +287,9 @@ struct Handle {
    double fp32_thr = 0.0;
    double next_bound = HUGE_VAL;    // bound of the next add_shell (reset by it)
    bool has_fp32[256];
+   // per-class kernel choice (libgint_autotune / libgint_set_tuning): primitive and group kernel
+   // variant, 0 = the generated per-lane kernels where the class has them, 1 = the per-warp ones
+   uint8_t tune_prim[256], tune_group[256];
    int S_of[256];                   // plans[c].S, kept compact for the streaming path
    bool plans_ready = false;
    // streaming state
@@ -306,6 +309,12 @@ struct Handle {
    struct RecBatch { DBuf rec; std::vector<RecSeg> segs; size_t ac_doubles = 0; };
    bool recording = false;
    std::vector<RecBatch> recs;
+   long long rec_gen = 0;           // bumped whenever the recording changes
+   // the replay captured as a CUDA graph, and what it was captured with
+   struct GraphKey { DevCtx ctx; long long rec_gen; void *ac, *gscr; size_t half; };
+   cudaGraphExec_t graph_exec = nullptr;
+   GraphKey graph_key;
+   long long graph_launches = 0;
    DBuf rec_ac, rec_gscr;
    // optional device event counters [256 classes][4]
    DBuf d_cnt;
@@ -646,6 +655,8 @@ static void flush(Handle *h) {
       char *base = dev_rec;
       bt.cls = g.c & 255;
       bt.fp32 = g.c >= kFp32;
+      bt.prim_variant = h->tune_prim[g.c & 255];
+      bt.group_variant = h->tune_group[g.c & 255];
       bt.plan = (const ClassPlan *)h->d_plans.p + (g.c & 255);
       bt.prm = (const uint32_t *)(base + g.o_prm);
       bt.prm_shell = (const uint32_t *)(base + g.o_ps);
@@ -787,41 +798,19 @@ static void set_K_impl(Handle *h, int nspin, const double *Ka, const double *Kb,
    }
 }
 
-// Re-run every recorded batch with the current P (K is zeroed first). Returns the elapsed
-// milliseconds measured with CUDA events on the handle's stream.
-static double replay_impl(Handle *h, double *kt, double *kcls = nullptr) {
-   if (h->err) return -1.0;
-   use_device(h);
-   if (h->recs.empty()) { set_error(h, 4, "libgint_replay: nothing recorded"); return -1.0; }
-   if (!upload_tables(h)) return -1.0;
-   size_t ac = 0, gs = 0;
-   for (auto &rb : h->recs) {
-      ac = std::max(ac, rb.ac_doubles);
-      for (auto &g : rb.segs) { int a, b; gs = std::max(gs, group_global_scratch(h->plans[g.c & 255], &a, &b)); }
-   }
-   // Every batch numbers its AC rows from 0, and the worker streams run the segments of
-   // consecutive batches at the same time, so batches alternate between two halves of the replay
-   // AC buffer (as the streamed build alternates two slots), and batch b + 2, which reuses batch b's
-   // half, starts on each worker only after every worker has finished batch b.
-   ac = (ac + 3) & ~(size_t)3;
-   if (!ensure(h, h->rec_ac, std::max<size_t>(2 * ac * 8, 256), "replay AC")) return -1.0;
-   if (gs && !ensure(h, h->rec_gscr, gs * 8, "replay HRR scratch")) return -1.0;
-   cudaEvent_t e0, e1;
-   cudaEventCreate(&e0); cudaEventCreate(&e1);
-   DevCtx ctx = make_ctx(h);
-   ck(h, cudaEventRecord(e0, h->stream), "event");
-   if (!h->team || !h->team->ok) { set_error(h, 4, "libgint_replay: call libgint_set_P first"); return -1.0; }
-   for (int sp = 0; sp < h->nspin; sp++) ck(h, cudaMemsetAsync(h->team->K[sp].p, 0, h->FP_size * 8, h->stream), "K zero");
-   // optional per-kernel timing: one event pair per launch, summed per kernel
-   std::vector<cudaEvent_t> kev;
-   std::vector<int> kcl;
+// Enqueue one replay of every recorded batch (K zeroed first) on the handle's stream: with
+// kt == nullptr the segments spread over the worker streams (forked from and joined back to the
+// handle's stream), otherwise they run in order on the handle's stream with an event before and
+// after each kernel (kev, kcl: per-kernel timing). ac is the replay AC buffer's half size.
+static bool enqueue_replay(Handle *h, const DevCtx &ctx, size_t ac, std::vector<cudaEvent_t> *kev,
+                           std::vector<int> *kcl, long long *nlaunch) {
+   for (int sp = 0; sp < h->nspin; sp++)
+      if (!ck(h, cudaMemsetAsync(h->team->K[sp].p, 0, h->FP_size * 8, h->stream), "K zero")) return false;
    auto kmark = [&]() {
-      if (!kt) return;
-      cudaEvent_t e; cudaEventCreate(&e); cudaEventRecord(e, h->stream); kev.push_back(e);
+      if (!kev) return;
+      cudaEvent_t e; cudaEventCreate(&e); cudaEventRecord(e, h->stream); kev->push_back(e);
    };
-   // per-kernel timing needs the launches in order on one stream; otherwise the segments spread
-   // over the worker streams
-   const bool spread = kt == nullptr;
+   const bool spread = kev == nullptr;
    if (spread) fork_workers(h);
    int nseg = 0;
    for (size_t bi = 0; bi < h->recs.size(); bi++) {
@@ -831,12 +820,14 @@ static double replay_impl(Handle *h, double *kt, double *kcls = nullptr) {
       if (spread && bi >= 2)
          for (int w = 0; w < kWorkStreams; w++)
             for (int w2 = 0; w2 < kWorkStreams; w2++)
-               ck(h, cudaStreamWaitEvent(h->work[w], h->batch_ev[bi & 1][w2], 0), "stream wait");
+               if (!ck(h, cudaStreamWaitEvent(h->work[w], h->batch_ev[bi & 1][w2], 0), "stream wait")) return false;
       for (auto &g : rb.segs) {
          BatchArgs bt;
          std::memset(&bt, 0, sizeof(bt));
          bt.cls = g.c & 255;
          bt.fp32 = g.c >= kFp32;
+         bt.prim_variant = h->tune_prim[g.c & 255];
+         bt.group_variant = h->tune_group[g.c & 255];
          bt.plan = (const ClassPlan *)h->d_plans.p + (g.c & 255);
          bt.prm = (const uint32_t *)(base + g.o_prm);
          bt.prm_shell = (const uint32_t *)(base + g.o_ps);
@@ -849,24 +840,72 @@ static double replay_impl(Handle *h, double *kt, double *kcls = nullptr) {
          bt.gscratch = (double *)h->rec_gscr.p;
          int a_, b_;
          const ClassPlan &hp = h->plans[g.c & 255];
-         cudaStream_t st = spread ? worker_for(h, nseg++, group_global_scratch(hp, &a_, &b_) != 0)
-                                  : h->stream;
+         cudaStream_t st = spread ? worker_for(h, nseg++, group_global_scratch(hp, &a_, &b_) != 0) : h->stream;
          kmark();
-         if (kt) kcl.push_back(g.c & 255);
-         if (!ck(h, launch_prim(ctx, bt, hp, st), "k_prim launch")) break;
+         if (kcl) kcl->push_back(g.c & 255);
+         if (!ck(h, launch_prim(ctx, bt, hp, st), "k_prim launch")) return false;
          kmark();
-         if (!ck(h, launch_group(ctx, bt, hp, st), "k_group launch")) break;
+         if (!ck(h, launch_group(ctx, bt, hp, st), "k_group launch")) return false;
          kmark();
-         h->n_launch += 2;
+         *nlaunch += 2;
       }
       if (spread)
          for (int w = 0; w < kWorkStreams; w++)
-            ck(h, cudaEventRecord(h->batch_ev[bi & 1][w], h->work[w]), "event record");
+            if (!ck(h, cudaEventRecord(h->batch_ev[bi & 1][w], h->work[w]), "event record")) return false;
    }
    if (spread) join_workers(h);
-   ck(h, cudaEventRecord(e1, h->stream), "event");
-   ck(h, cudaEventSynchronize(e1), "replay");
+   return !h->err;
+}
+
+static void drop_graph(Handle *h) {
+   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+   h->graph_exec = nullptr;
+}
+
+// Re-run every recorded batch with the current P (K is zeroed first). Returns the elapsed
+// milliseconds measured with CUDA events on the handle's stream. The spread replay is captured
+// once into a CUDA graph (the whole K build: every class segment's two kernels on the worker
+// streams, with their batch-to-batch dependencies) and relaunched as one graph while the recording
+// and the device pointers it was captured with stay the same.
+// Checks that a replay can run and sizes its buffers; *half = the AC buffer's half size.
+static bool prepare_replay(Handle *h, size_t *half) {
+   if (h->err) return false;
+   use_device(h);
+   if (h->recs.empty()) { set_error(h, 4, "libgint_replay: nothing recorded"); return false; }
+   if (!h->team || !h->team->ok) { set_error(h, 4, "libgint_replay: call libgint_set_P first"); return false; }
+   if (!upload_tables(h)) return false;
+   size_t ac = 0, gs = 0;
+   for (auto &rb : h->recs) {
+      ac = std::max(ac, rb.ac_doubles);
+      for (auto &g : rb.segs) { int a, b; gs = std::max(gs, group_global_scratch(h->plans[g.c & 255], &a, &b)); }
+   }
+   // Every batch numbers its AC rows from 0, and the worker streams run the segments of
+   // consecutive batches at the same time, so batches alternate between two halves of the replay
+   // AC buffer (as the streamed build alternates two slots), and batch b + 2, which reuses batch b's
+   // half, starts on each worker only after every worker has finished batch b. A recording of one
+   // batch needs one half.
+   ac = (ac + 3) & ~(size_t)3;
+   const size_t halves = h->recs.size() > 1 ? 2 : 1;
+   if (!ensure(h, h->rec_ac, std::max<size_t>(halves * ac * 8, 256), "replay AC")) return false;
+   if (gs && !ensure(h, h->rec_gscr, gs * 8, "replay HRR scratch")) return false;
+   *half = ac;
+   return true;
+}
+
+static double replay_impl(Handle *h, double *kt, double *kcls = nullptr) {
+   size_t ac = 0;
+   if (!prepare_replay(h, &ac)) return -1.0;
+   DevCtx ctx = make_ctx(h);
+   cudaEvent_t e0, e1;
+   cudaEventCreate(&e0); cudaEventCreate(&e1);
    if (kt) {
+      // per-kernel timing: the launches in order on one stream, one event pair per kernel
+      std::vector<cudaEvent_t> kev;
+      std::vector<int> kcl;
+      ck(h, cudaEventRecord(e0, h->stream), "event");
+      enqueue_replay(h, ctx, ac, &kev, &kcl, &h->n_launch);
+      ck(h, cudaEventRecord(e1, h->stream), "event");
+      ck(h, cudaEventSynchronize(e1), "replay");
       kt[0] = kt[1] = 0.0;
       if (kcls) std::memset(kcls, 0, sizeof(double) * 512);
       for (size_t i = 0; i + 2 < kev.size(); i += 3) {
@@ -877,11 +916,111 @@ static double replay_impl(Handle *h, double *kt, double *kcls = nullptr) {
          if (kcls) { kcls[kcl[i / 3] * 2] += a; kcls[kcl[i / 3] * 2 + 1] += b; }
       }
       for (auto e : kev) cudaEventDestroy(e);
+   } else {
+      Handle::GraphKey key;
+      std::memset(&key, 0, sizeof(key));
+      std::memcpy(&key.ctx, &ctx, sizeof(ctx));
+      key.rec_gen = h->rec_gen;
+      key.ac = h->rec_ac.p; key.gscr = h->rec_gscr.p; key.half = ac;
+      if (!h->graph_exec || std::memcmp(&key, &h->graph_key, sizeof(key)) != 0) {
+         drop_graph(h);
+         cudaGraph_t graph = nullptr;
+         long long n = 0;
+         bool ok = ck(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "graph capture");
+         if (ok) {
+            ok = enqueue_replay(h, ctx, ac, nullptr, nullptr, &n);
+            const cudaError_t ec = cudaStreamEndCapture(h->stream, &graph);
+            ok = ok && ck(h, ec, "graph capture");
+         }
+         if (ok && !ck(h, cudaGraphInstantiate(&h->graph_exec, graph, 0), "graph instantiate")) h->graph_exec = nullptr;
+         if (graph) cudaGraphDestroy(graph);
+         if (!h->graph_exec) { cudaEventDestroy(e0); cudaEventDestroy(e1); return -1.0; }
+         h->graph_key = key;
+         h->graph_launches = n;
+      }
+      ck(h, cudaEventRecord(e0, h->stream), "event");
+      ck(h, cudaGraphLaunch(h->graph_exec, h->stream), "graph launch");
+      h->n_launch += h->graph_launches;
+      ck(h, cudaEventRecord(e1, h->stream), "event");
+      ck(h, cudaEventSynchronize(e1), "replay");
    }
    float ms = -1.f;
    cudaEventElapsedTime(&ms, e0, e1);
    cudaEventDestroy(e0); cudaEventDestroy(e1);
    return h->err ? -1.0 : (double)ms;
+}
+
+// The autotuner: for every class of the recording, the primitive kernels (generated per-lane VRR,
+// variant 0, against the per-warp interpreted VRR, variant 1) and the group kernels (one lane per
+// contraction row with generated HRR, variant 0, against one warp per row with the interpreted HRR,
+// variant 1) are timed on the class's recorded segments, serialised on the handle's stream with
+// CUDA events, and the faster of each is kept. FP32 segments have only variant 0. K is zeroed
+// afterwards (the timing runs add into it).
+static int autotune_impl(Handle *h, int *out) {
+   size_t ac = 0;
+   if (!prepare_replay(h, &ac)) return h->err ? h->err : 4;
+   drop_graph(h);
+   DevCtx ctx = make_ctx(h);
+   double t[256][2][2] = {};
+   bool seen[256] = {}, alt_p[256] = {}, alt_g[256] = {};
+   cudaEvent_t ev[5];
+   for (auto &e : ev) cudaEventCreate(&e);
+   for (size_t bi = 0; bi < h->recs.size() && !h->err; bi++) {
+      auto &rb = h->recs[bi];
+      char *base = (char *)rb.rec.p;
+      double *ac_half = (double *)h->rec_ac.p + (bi & 1) * ac;
+      for (auto &g : rb.segs) {
+         if (g.c >= kFp32) continue;
+         const int c = g.c;
+         const ClassPlan &hp = h->plans[c];
+         BatchArgs bt;
+         std::memset(&bt, 0, sizeof(bt));
+         bt.cls = c;
+         bt.plan = (const ClassPlan *)h->d_plans.p + c;
+         bt.prm = (const uint32_t *)(base + g.o_prm);
+         bt.prm_shell = (const uint32_t *)(base + g.o_ps);
+         bt.shells = (const ShellRec *)(base + g.o_sh);
+         bt.groups = (const GroupRec *)(base + g.o_g);
+         bt.qrtts = (const QrttRec *)(base + g.o_q);
+         bt.rowgrp = (const uint32_t *)(base + g.o_rg);
+         bt.nprm = g.nprm; bt.nshell = g.nshell; bt.ngroup = g.ngroup; bt.nqrtt = g.nqrtt;
+         bt.AC = ac_half + g.ac_off;
+         bt.gscratch = (double *)h->rec_gscr.p;
+         const int cl[4] = {c >> 6, (c >> 4) & 3, (c >> 2) & 3, c & 3};
+         seen[c] = true;
+         alt_p[c] = prim_has_generated(c);
+         alt_g[c] = class_has_fp32(cl[0], cl[1], cl[2], cl[3]);
+         ck(h, cudaEventRecord(ev[0], h->stream), "event");
+         bt.prim_variant = 1;
+         ck(h, launch_prim(ctx, bt, hp, h->stream), "k_prim launch");
+         ck(h, cudaEventRecord(ev[1], h->stream), "event");
+         bt.prim_variant = 0;
+         ck(h, launch_prim(ctx, bt, hp, h->stream), "k_prim launch");
+         ck(h, cudaEventRecord(ev[2], h->stream), "event");
+         bt.group_variant = 1;
+         ck(h, launch_group(ctx, bt, hp, h->stream), "k_group launch");
+         ck(h, cudaEventRecord(ev[3], h->stream), "event");
+         bt.group_variant = 0;
+         ck(h, launch_group(ctx, bt, hp, h->stream), "k_group launch");
+         ck(h, cudaEventRecord(ev[4], h->stream), "event");
+         if (!ck(h, cudaEventSynchronize(ev[4]), "autotune")) break;
+         float ms[4];
+         for (int k = 0; k < 4; k++) cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]);
+         t[c][0][1] += ms[0]; t[c][0][0] += ms[1]; t[c][1][1] += ms[2]; t[c][1][0] += ms[3];
+      }
+   }
+   for (auto &e : ev) cudaEventDestroy(e);
+   for (int sp = 0; sp < h->nspin; sp++) ck(h, cudaMemsetAsync(h->team->K[sp].p, 0, h->FP_size * 8, h->stream), "K zero");
+   ck(h, cudaStreamSynchronize(h->stream), "autotune");
+   if (h->err) return h->err;
+   for (int c = 0; c < 256; c++) {
+      if (!seen[c]) continue;
+      h->tune_prim[c] = (alt_p[c] && t[c][0][1] < t[c][0][0]) ? 1 : 0;
+      h->tune_group[c] = (alt_g[c] && t[c][1][1] < t[c][1][0]) ? 1 : 0;
+   }
+   if (out)
+      for (int c = 0; c < 256; c++) { out[2 * c] = h->tune_prim[c]; out[2 * c + 1] = h->tune_group[c]; }
+   return 0;
 }
 
 }  // namespace gint
@@ -902,6 +1041,7 @@ void *libgint_create_handle(void) {
       build_vops(h->plans[c], h->vops);
       h->S_of[c] = h->plans[c].S;
       h->has_fp32[c] = class_has_fp32(c >> 6, (c >> 4) & 3, (c >> 2) & 3, c & 3);
+      h->tune_prim[c] = h->tune_group[c] = 0;
    }
    return h;
 }
@@ -1165,6 +1305,77 @@ void libgint_add_qrtt(void *hh, double symm_fac, int la, int lb, int lc, int ld,
    if (o32) { h->q[cl + kFp32].qrtts.push_back(r); o32->nq++; }   // the FP32 group updates the same rows
 }
 
+}  // extern "C"
+
+namespace gint {
+
+// Primitive-target products per contraction row above which a group is split (see commit_group).
+constexpr size_t kChunkWork = 4096;
+
+// Commits the group of one set quartet and queue class: its shell quartets [shell0, end of the
+// shell queue), primitives [prm0, end) and contraction rows [qrtt0, qrtt0 + nrows). The group
+// kernels give each contraction row to one lane (or warp), which contracts every primitive of every
+// shell of the group, so one heavy group keeps one lane busy long after the rest of the GPU has
+// finished (a (pp|ps) group of 8-primitive sets holds up to 8192 primitive quartets per image
+// pair). A group with more than kChunkWork primitive-target products per row is therefore
+// committed as several groups over consecutive chunks of its primitives: each chunk gets shell
+// records of its own that cover sub-ranges of the shells' primitive lists (the original records
+// stay for the primitive kernel) and its own copy of the rows. Contraction, HRR, spherical
+// transform and K update are linear, so the chunks' K updates add up to the group's.
+static void commit_group(Handle *h, ClassQ &Q, int qcls, uint32_t shell0, uint32_t qrtt0, size_t prm0,
+                         const uint8_t nl[4], int nrows) {
+   const uint32_t nshell = (uint32_t)Q.shells.size() - shell0;
+   const size_t nprm = Q.prm.size() - prm0;
+   const size_t S = (size_t)h->S_of[qcls & 255];
+   const size_t cap = std::max<size_t>(32, kChunkWork / std::max<size_t>(S, 1));
+   size_t recs = nprm * 8 + (size_t)nshell * sizeof(ShellRec);
+   auto push_group = [&](uint32_t sh_off, uint32_t nsh, uint32_t q_off) {
+      GroupRec g;
+      g.shell_off = sh_off; g.nshell = nsh; g.qrtt_off = q_off;
+      for (int q = 0; q < 4; q++) g.nl[q] = nl[q];
+      Q.groups.push_back(g);
+      recs += sizeof(GroupRec) + (size_t)nrows * sizeof(QrttRec);
+   };
+   if (nprm <= cap) {
+      push_group(shell0, nshell, qrtt0);
+   } else {
+      QrttRec rows[kMaxNl * kMaxNl * kMaxNl * kMaxNl];
+      std::memcpy(rows, Q.qrtts.data() + qrtt0, sizeof(QrttRec) * (size_t)nrows);
+      uint32_t chunk_shell0 = (uint32_t)Q.shells.size(), q_off = qrtt0;
+      size_t in_chunk = 0;
+      for (uint32_t si = shell0; si < shell0 + nshell; si++) {
+         const ShellRec sr = Q.shells.data()[si];
+         for (uint32_t p = 0; p < sr.nprm;) {
+            const uint32_t take = (uint32_t)std::min<size_t>(sr.nprm - p, cap - in_chunk);
+            ShellRec c = sr;
+            c.prm_off = sr.prm_off + p;
+            c.nprm = take;
+            Q.shells.push_back(c);
+            recs += sizeof(ShellRec);
+            p += take;
+            in_chunk += take;
+            if (in_chunk == cap) {
+               push_group(chunk_shell0, (uint32_t)Q.shells.size() - chunk_shell0, q_off);
+               chunk_shell0 = (uint32_t)Q.shells.size();
+               in_chunk = 0;
+               q_off = (uint32_t)Q.qrtts.size();
+               Q.qrtts.append(rows, (size_t)nrows);
+            }
+         }
+      }
+      if (in_chunk > 0) push_group(chunk_shell0, (uint32_t)Q.shells.size() - chunk_shell0, q_off);
+      else Q.qrtts.resize(q_off);   // the last copy of the rows has no chunk
+   }
+   if (!Q.active) { Q.active = true; h->active.push_back(qcls); }
+   h->pend_prims += nprm;
+   h->pend_ac += nprm * S;
+   h->pend_rec += recs;
+}
+
+}  // namespace gint
+
+extern "C" {
+
 void libgint_add_set(void *hh) {
    Handle *h = (Handle *)hh;
    for (int o = 0; o < h->nopen; o++) {
@@ -1183,17 +1394,7 @@ void libgint_add_set(void *hh) {
          Q.qrtts.resize(og.qrtt_off);
          continue;
       }
-      GroupRec g;
-      g.shell_off = og.shell_off;
-      g.nshell = nshell;
-      g.qrtt_off = og.qrtt_off;
-      for (int q = 0; q < 4; q++) g.nl[q] = og.nl[q];
-      Q.groups.push_back(g);
-      if (!Q.active) { Q.active = true; h->active.push_back(og.cls); }
-      const size_t added = Q.prm.size() - og.prm_off;
-      h->pend_prims += added;
-      h->pend_ac += added * (size_t)h->S_of[og.cls & 255];
-      h->pend_rec += added * 8 + nshell * sizeof(ShellRec) + sizeof(GroupRec) + nrows * sizeof(QrttRec);
+      commit_group(h, Q, og.cls, og.shell_off, og.qrtt_off, og.prm_off, og.nl, nrows);
    }
    h->nopen = 0;
    const size_t budget = slot_budget_bytes(h);
@@ -1276,15 +1477,9 @@ int libgint_add_set_quartets(void *hh, int n, const int *sets, const int *shell_
             iqrt++;
             const uint32_t nshell = (uint32_t)Q.shells.size() - shell0;
             if (nshell > 0) {
-               GroupRec g;
-               g.shell_off = shell0; g.nshell = nshell; g.qrtt_off = qrtt0;
-               for (int u = 0; u < 4; u++) g.nl[u] = (uint8_t)r[4 + u];
-               Q.groups.push_back(g);
-               if (!Q.active) { Q.active = true; h->active.push_back(cl); }
-               const size_t added = Q.prm.size() - prm0;
-               h->pend_prims += added;
-               h->pend_ac += added * (size_t)h->S_of[cl];
-               h->pend_rec += added * 8 + nshell * sizeof(ShellRec) + sizeof(GroupRec) + nrow * sizeof(QrttRec);
+               uint8_t nl4[4];
+               for (int u = 0; u < 4; u++) nl4[u] = (uint8_t)r[4 + u];
+               commit_group(h, Q, cl, shell0, qrtt0, prm0, nl4, nrow);
             } else {
                Q.qrtts.resize(qrtt0);   // nothing to compute: the group rolls back, as in add_set
             }
@@ -1352,15 +1547,39 @@ void libgint_record(void *hh, int on) {
    Handle *h = (Handle *)hh;
    if (on) {
       drain(h);
+      drop_graph(h);
       for (auto &rb : h->recs) release(rb.rec);
       h->recs.clear();
    } else {
       flush(h);
    }
    h->recording = on != 0;
+   h->rec_gen++;
 }
 
 double libgint_replay(void *hh) { return replay_impl((Handle *)hh, nullptr); }
+
+// The per-class kernel choice (no counterpart in the reference): libgint_autotune times both
+// primitive kernels and both group kernels of every class on the recorded quartet list (after
+// libgint_record and libgint_set_P) and keeps the faster ones for every following launch;
+// out[2c], out[2c+1] (if out is given) receive class c's choices. libgint_set_tuning installs a
+// table of the same layout (e.g. one measured earlier); libgint_get_tuning reads the current one.
+int libgint_autotune(void *hh, int *out) { return autotune_impl((Handle *)hh, out); }
+
+void libgint_set_tuning(void *hh, const int *in) {
+   Handle *h = (Handle *)hh;
+   drop_graph(h);
+   for (int c = 0; c < 256; c++) {
+      const int cl[4] = {c >> 6, (c >> 4) & 3, (c >> 2) & 3, c & 3};
+      h->tune_prim[c] = in[2 * c] ? 1 : 0;
+      h->tune_group[c] = (in[2 * c + 1] && class_has_fp32(cl[0], cl[1], cl[2], cl[3])) ? 1 : 0;
+   }
+}
+
+void libgint_get_tuning(void *hh, int *out) {
+   Handle *h = (Handle *)hh;
+   for (int c = 0; c < 256; c++) { out[2 * c] = h->tune_prim[c]; out[2 * c + 1] = h->tune_group[c]; }
+}
 
 // Recompute K from the recorded quartet list into caller-owned device buffers, without any
 // device allocation: the primitive-quartet intermediates and the HRR workspace live in the
@@ -1432,6 +1651,8 @@ int libgint_replay_noalloc(void *hh, const double *P_dev, double *K_dev, size_t 
          std::memset(&bt, 0, sizeof(bt));
          bt.cls = g.c & 255;
          bt.fp32 = g.c >= kFp32;
+         bt.prim_variant = h->tune_prim[g.c & 255];
+         bt.group_variant = h->tune_group[g.c & 255];
          bt.plan = (const ClassPlan *)h->d_plans.p + (g.c & 255);
          bt.prm = (const uint32_t *)(base + g.o_prm);
          bt.prm_shell = (const uint32_t *)(base + g.o_ps);
@@ -1585,6 +1806,7 @@ void libgint_destroy_handle(void *hh) {
    Handle *h = (Handle *)hh;
    if (!h) return;
    if (h->stream) { use_device(h); cudaStreamSynchronize(h->stream); }
+   drop_graph(h);
    for (Slot &s : h->slots) {
       release(s.rec); release(s.ac); release(s.gscr);
       if (s.ev) cudaEventDestroy(s.ev);

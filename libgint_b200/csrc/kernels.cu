@@ -854,7 +854,7 @@ static bool prim2_lane(const ClassPlan &hp) { return hp.V <= 96; }
 // then the team kernel for the largest classes.
 cudaError_t launch_prim(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan &hp, cudaStream_t st) {
    if (bt.nprm == 0) return cudaSuccess;
-   {
+   if (bt.prim_variant == 0 || bt.fp32) {
       cudaError_t err = cudaSuccess;
       if (prim3_launch(ctx, bt, st, &err)) return err;
    }
@@ -917,13 +917,13 @@ size_t group_global_scratch(const ClassPlan &hp, int *grid, int *warps) {
 // then k_group_lane / k_group.
 cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan &hp, cudaStream_t st) {
    if (bt.nqrtt == 0) return cudaSuccess;
-   {
+   if (bt.group_variant == 0 || bt.fp32) {
       cudaError_t err = cudaSuccess;
       if (group3_launch(ctx, bt, st, &err)) return err;
    }
    if (bt.fp32) return cudaErrorInvalidValue;   // FP32 segments exist only for classes with k_group3
    const size_t wd = group_warp_doubles(hp);
-   if (wd <= 40) {
+   if (wd <= 40 && bt.group_variant == 0) {
       // small workspace: one lane per group, 32 groups per warp
       const int lane_doubles = (int)wd;
       const size_t plan_bytes = group_hdr_bytes();

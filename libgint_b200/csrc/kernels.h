@@ -60,6 +60,8 @@ struct BatchArgs {
    int fp32;                  // 1: the segment's shell quartets run in FP32 (Fm, VRR, contraction, HRR)
    double *gscratch;          // HRR workspace in global memory for the largest classes
    int cls;                   // la*64 + lb*16 + lc*4 + ld
+   int prim_variant;          // 0: k_prim3 where the class has it (lane per image); 1: k_prim2 (warp per image)
+   int group_variant;         // 0: k_group3 where the class has it (lane per row); 1: k_group (warp per row)
 };
 
 bool build_class_plan(int la, int lb, int lc, int ld, ClassPlan &p);
@@ -70,6 +72,8 @@ cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan
 size_t group_global_scratch(const ClassPlan &hp, int *grid, int *warps);
 constexpr int kGroupKpDoubles = 32;   // per-warp shared buffer of contraction coefficients in k_group
 int prim_team_size(const ClassPlan &hp);
+// whether k_prim3 (generated VRR) covers class cls (prim3.cu)
+bool prim_has_generated(int cls);
 // classes with an FP32 path (generated VRR and HRR code): la + lb + lc + ld <= 3
 constexpr bool class_has_fp32(int la, int lb, int lc, int ld) { return la + lb + lc + ld <= 3; }
 // Fixed device scratch (file-scope device array in kernels.cu) used by libgint_replay_noalloc:

@@ -335,6 +335,12 @@ bool PRIM3_CAT(prim3_launch_part, PRIM3_PART)(const DevCtx &ctx, const BatchArgs
 cudaError_t PRIM3_CAT(prim3_preload_part, PRIM3_PART)(int smax) { return PartPreload<PRIM3_PART>::run(smax); }
 
 #if PRIM3_PART == 0
+bool prim_has_generated(int cls) {
+   for (int i = 0; i < kVrrGenCount; i++)
+      if (kVrrGenClasses[i] == cls) return true;
+   return false;
+}
+
 cudaError_t prim3_preload(int smax) {
    cudaError_t (*parts[])(int) = {prim3_preload_part0, prim3_preload_part1, prim3_preload_part2, prim3_preload_part3,
                                prim3_preload_part4, prim3_preload_part5, prim3_preload_part6, prim3_preload_part7};

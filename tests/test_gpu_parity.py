@@ -292,3 +292,45 @@ def test_bulk_submission_matches_oracle(engine_so, oracle_path):
     assert code_b == 0
     assert_fp64_parity(Kb, Ko, magnitude_K(oracle_path, wl), wl, "bulk submission: ")
     assert_same_decisions(cb, co, wl)
+
+
+@pytest.mark.gpu
+def test_autotuned_graph_replay_matches_oracle(engine_so, oracle_path):
+    """The replay as a CUDA graph with the autotuner's per-class kernel choice: the oracle's K, with
+    the same screening decisions, for every choice table (the tuned one, all per-warp, all per-lane);
+    a second replay relaunches the captured graph."""
+    from libgint_b200.capi import load_engine
+    lib = load_engine()
+    wl = Workload("periodic_l3", n_mol=2, box_ang=6.5, n_img_1d=3, n_occ=16, max_prm=4, max_ncontr=3)
+    Ko, _, _, co = _k(oracle_path, wl, counters=True)
+    Kabs = magnitude_K(oracle_path, wl)
+    s = Session(Api(engine_so), wl)
+    h = ctypes.c_void_p(s.h)
+    lib.libgint_record(h, 1)
+    s.build_K()
+    lib.libgint_record(h, 0)
+    P = wl.Pflat
+    D = ctypes.POINTER(ctypes.c_double)
+    lib.libgint_set_P(h, P.ctypes.data_as(D), P.size)
+    table = (ctypes.c_int * 512)()
+    assert lib.libgint_autotune(h, table) == 0, lib.libgint_error_string(h)
+    tuned = np.array(table).reshape(256, 2)
+    print(f"autotune: per-warp primitive kernel for {int(tuned[:, 0].sum())} classes, per-warp group kernel "
+          f"for {int(tuned[:, 1].sum())}")
+    K = np.zeros(P.size)
+    for label, tab in [("tuned", tuned), ("per-warp", np.ones((256, 2), dtype=np.int32)),
+                       ("per-lane", np.zeros((256, 2), dtype=np.int32))]:
+        t = np.ascontiguousarray(tab, dtype=np.int32)
+        lib.libgint_set_tuning(h, t.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+        lib.libgint_set_counters(h, 1)
+        for _ in range(2):
+            assert lib.libgint_replay(h) > 0, lib.libgint_error_string(h)
+        buf = (ctypes.c_ulonglong * 1024)()
+        lib.libgint_get_counters(h, buf)
+        lib.libgint_set_counters(h, 0)
+        lib.libgint_get_K(h, K.ctypes.data_as(D))
+        assert lib.libgint_last_error(h) == 0
+        assert_fp64_parity(K, Ko, Kabs, wl, f"graph replay, {label} kernels: ")
+        ce = np.frombuffer(buf, dtype=np.uint64).reshape(256, 4) // 2   # two replays counted
+        assert_same_decisions(ce, co, wl)
+    s.close()
