@@ -11,15 +11,20 @@ from a hashed offset), so that a step takes about a second; the sample is named 
 config.workload.
 
 One step = one K build over the sample's screened quartet list:
-  value  device-resident throughput: the quartet list recorded on the GPU (libgint_record) and K
-         recomputed from it (libgint_replay: zero K, every kernel), timed with CUDA events on the
-         engine's stream; shell quartets per second over all ranks.
-  e2e    the same metric through the C-ABI as CP2K drives it: an OpenMP team of --host-threads
+  value  device-resident throughput of the mixed-precision, batched build: shell quartets whose
+         Schwarz bound is below --fp32-threshold (1e-5) run in FP32 (classes with
+         la+lb+lc+ld <= 3), the quartet list is recorded on the GPU (libgint_record, few large
+         batches) and K is recomputed from it as one CUDA graph (libgint_replay) with the per-class
+         kernels chosen by libgint_autotune; CUDA events on the engine's stream; shell quartets per
+         second over all ranks. The same all-FP64 build is timed beside it ("fp64"), with the
+         mixed build's max|dK| and |dE_x| against it.
+  e2e    the mixed build through the C-ABI as CP2K drives it: an OpenMP team of --host-threads
          threads with one handle each, every thread streaming its share of the set quartets
-         (libgint_set_P from host memory, the add_* calls, libgint_get_K into one shared host K);
-         set_P and get_K are collective over the team.
+         (libgint_set_P from host memory, the add_* calls with each shell quartet's bound,
+         libgint_get_K into one shared host K); set_P and get_K are collective over the team.
 The reference arm (--impl reference) times the CPU restatement of the path (the oracle) on the host
-cores over a strided sub-sample of the same workload.
+cores over a strided sub-sample of the same workload. The reference's own CUDA library is timed on
+a small sample of the workload beside ours ("reference_cuda").
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -67,7 +72,14 @@ def parse():
                     help="OpenMP team size of the end-to-end leg (one handle per thread)")
     ap.add_argument("--device-only", action="store_true",
                     help="record and replay only (no end-to-end, CPU or reference legs)")
-    ap.add_argument("--max-mem-mb", type=int, default=7000, help="libgint_set_max_mem of the recording handle")
+    ap.add_argument("--max-mem-mb", type=int, default=40000,
+                    help="libgint_set_max_mem of the recording handle (large: few batches, one launch per class each)")
+    ap.add_argument("--clusters-stride", type=int, default=64,
+                    help="set-quartet sample of the batched-systems leg (0 = skip the leg)")
+    ap.add_argument("--scf-stride", type=int, default=1 << 14,
+                    help="set-quartet sample of the SCF-loop leg (0 = skip the leg)")
+    ap.add_argument("--fp32-threshold", type=float, default=1e-5,
+                    help="Schwarz bound below which shell quartets run in FP32 (the mixed path)")
     ap.add_argument("--host-mem-mb", type=int, default=300,
                     help="libgint_set_max_mem of each end-to-end handle (smaller batches start the GPU sooner)")
     ap.add_argument("--no-reference-cuda", action="store_true",
@@ -211,6 +223,111 @@ def group_flops(lib, wl):
     return float(np.sum(rows * (sq[:, 5] * f[:, 4] + sq[:, 4] * f[:, 5] + f[:, 6] + f[:, 7])))
 
 
+def scf_leg(args, lib, api):
+    """The SCF-loop workload (128 molecules, 15.6 A cell, the 256 nearest image cells, l <= 3 basis),
+    on a uniform 1/--scf-stride sample of its set quartets: the quartet list is recorded once with
+    P_0 (mixed precision, --max-mem-mb 7000 recording budget), then 10 K updates follow
+    P_k = P_0 + eps_k sym(N(0,1)), eps_k log-spaced from 1e-2 to 1e-6, each one
+    K_k = K_{k-1} + K(P_k - P_{k-1}) from the recording with incremental dP screening at the Schwarz
+    threshold 1e-11 (libgint_replay_incremental, one CUDA graph). Device time per iteration; the
+    last K against a full replay with P_10."""
+    import torch
+    from libgint_b200.workload import Session, Workload, set_fp32_threshold
+    D = ctypes.POINTER(ctypes.c_double)
+    t0 = time.perf_counter()
+    wl = Workload("periodic_l3_scf", setq_stride=args.scf_stride)
+    gen_s = time.perf_counter() - t0
+    free0, total = torch.cuda.mem_get_info()
+    set_fp32_threshold(args.fp32_threshold)
+    try:
+        s = Session(api, wl, max_mem_mb=7000)
+        h = ctypes.c_void_p(s.h)
+        lib.libgint_record(h, 1)
+        K, _, _ = s.build_K()
+        lib.libgint_record(h, 0)
+    finally:
+        set_fp32_threshold(0.0)
+    lib.libgint_autotune(h, None)
+    free1, _ = torch.cuda.mem_get_info()
+    rng = np.random.default_rng(5)
+    P0 = wl.Pflat
+    P = P0.copy()
+    eps = np.logspace(-2, -6, 10)
+    iters = []
+    for k, e in enumerate(eps):
+        A = rng.standard_normal((wl.n_bf, wl.n_bf))
+        Pk = P0 + e * wl.pack(0.5 * (A + A.T))
+        dP = Pk - P
+        lib.libgint_set_P(h, dP.ctypes.data_as(D), dP.size)
+        lib.libgint_set_K(h, K.ctypes.data_as(D), K.size)
+        ms = lib.libgint_replay_incremental(h, 1e-11)
+        lib.libgint_get_K(h, K.ctypes.data_as(D))
+        iters.append(ms)
+        P = Pk
+    err = lib.libgint_last_error(h)
+    # the last K against a full build (replay without screening) with P_10
+    lib.libgint_set_P(h, P.ctypes.data_as(D), P.size)
+    full_ms = lib.libgint_replay(h)
+    Kf = np.zeros_like(K)
+    lib.libgint_get_K(h, Kf.ctypes.data_as(D))
+    s.close()
+    return {"workload": f"periodic_l3_scf: 128 water-like molecules, 15.6 A cell, the 256 image cells nearest the "
+                        f"origin, l<=3 basis as periodic_l3; a uniform 1/{args.scf_stride} sample of the set "
+                        f"quartets ({wl.info['n_setq']} set quartets, {wl.info['n_shells']} shell quartets, "
+                        f"{wl.info['n_prims']} primitive quartets)",
+            "generation_s": gen_s, "error": int(err),
+            "ms_per_scf_iter": float(np.mean(iters)), "iteration_ms": [float(x) for x in iters],
+            "full_build_ms": full_ms, "eps": [float(x) for x in eps],
+            "final_max_dK_vs_full_build": float(np.abs(K - Kf).max()),
+            "final_abs_dEx_vs_full_build": abs(wl.exchange_energy(K) - wl.exchange_energy(Kf)),
+            "device_mem_mb_held_after_recording": (free0 - free1) / 2**20,
+            "device_mem_cap_mb": 7000}
+
+
+def clusters_leg(args, lib, api):
+    """The batched-systems workload: 96 independent non-periodic water clusters of 2-24 molecules
+    (uniform, one seed per system), alternating l <= 2 and l <= 3 bases, all in one handle, on a
+    uniform 1/--clusters-stride sample of each system's set quartets: one recording of all systems'
+    quartets (one class-sorted list) replayed as one CUDA graph with autotuned kernels, FP64 and
+    mixed precision."""
+    from libgint_b200.workload import cluster_batch, set_fp32_threshold
+    t0 = time.perf_counter()
+    b = cluster_batch(96, seed=0, setq_stride=args.clusters_stride)
+    gen_s = time.perf_counter() - t0
+    out = {"workload": f"96 water clusters of 2-24 molecules (l<=2 and l<=3 bases alternating), one handle; a "
+                       f"uniform 1/{args.clusters_stride} sample of each system's set quartets "
+                       f"({b.info['n_setq']} set quartets, {b.info['n_shells']} shell quartets, "
+                       f"{b.info['n_prims']} primitive quartets, {b.info['n_sets']} sets)",
+           "generation_s": gen_s}
+    Ks = {}
+    for name, thr in (("fp64", 0.0), ("mixed", args.fp32_threshold)):
+        set_fp32_threshold(thr)
+        try:
+            h = b.setup(api, args.max_mem_mb)
+            hv = ctypes.c_void_p(h)
+            lib.libgint_record(hv, 1)
+            b.build_K(api, h)
+            lib.libgint_record(hv, 0)
+        finally:
+            set_fp32_threshold(0.0)
+        lib.libgint_autotune(hv, None)
+        for _ in range(args.warmup):
+            lib.libgint_replay(hv)
+        ms = float(np.mean([lib.libgint_replay(hv) for _ in range(args.steps)]))
+        K = np.zeros(int(b.offsets[-1]))
+        lib.libgint_get_K(hv, K.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        lib.libgint_get_stats(hv, (ctypes.c_longlong * 8)())
+        err = lib.libgint_last_error(hv)
+        lib.libgint_destroy_handle(hv)
+        Ks[name] = b.split(K)
+        out[name] = {"ms_per_step": ms, "value": b.info["n_shells"] / (ms / 1e3), "unit": UNIT, "error": int(err)}
+    out["mixed_max_dK_vs_fp64"] = max(float(np.abs(a - c).max()) for a, c in zip(Ks["mixed"], Ks["fp64"]))
+    out["mixed_max_abs_dEx_vs_fp64"] = float(np.max(np.abs(b.exchange_energies(Ks["mixed"]) -
+                                                            b.exchange_energies(Ks["fp64"]))))
+    out["mixed_speedup_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    return out
+
+
 def reference_cuda_leg(timeout_s=600):
     """The reference's own CUDA library (compiled unchanged from its sources for sm_100a) through the
     same C-ABI call stream, on a sample of the workload it can run: its encode_shell asserts
@@ -246,7 +363,7 @@ print("REFJSON" + json.dumps(out))
 def run_ours(args, world, rank, local):
     import torch
     from libgint_b200.capi import engine_path, load_engine
-    from libgint_b200.workload import Api, MultiSession, Session
+    from libgint_b200.workload import Api, MultiSession, Session, set_fp32_threshold
 
     torch.cuda.set_device(local)
     pg = False
@@ -265,11 +382,10 @@ def run_ours(args, world, rank, local):
     idx = np.arange(rank, nq, world)            # this rank's share of the set quartets
     total_shells = int(setq[:, 4].sum())
     api = Api(engine_path())
-    sess = Session(api, wl, max_mem_mb=args.max_mem_mb)
-    h = ctypes.c_void_p(sess.h)
     stats = (ctypes.c_longlong * 8)()
+    D = ctypes.POINTER(ctypes.c_double)
 
-    def check(hh=h):
+    def check(hh):
         e = lib.libgint_last_error(hh)
         if e:
             raise RuntimeError(f"engine error {e}: {lib.libgint_error_string(hh).decode()}")
@@ -293,53 +409,74 @@ def run_ours(args, world, rank, local):
         torch.distributed.all_reduce(t)
         return t.cpu().numpy()
 
-    # 1) first K build through the C-ABI, recording the device-resident quartet list
-    lib.libgint_record(h, 1)
-    K0, ms_rec, _ = sess.build_K_subset(idx)
-    lib.libgint_record(h, 0)
-    check()
-    lib.libgint_get_stats(h, stats)
-    rec_bytes = int(stats[5])
-    K0_local = K0.copy()
-    K0 = sum_K(K0)
-
-    # 2) value: device-resident K builds (replay), timed with CUDA events on the engine stream
-    for _ in range(args.warmup):
-        lib.libgint_replay(h)
-    barrier()
-    lib.libgint_get_stats(h, stats)
-    launches0 = stats[4]
     clocks = ClockSampler(local)
-    clocks.start()
-    step_ms = []
-    for _ in range(args.steps):
-        step_ms.append(lib.libgint_replay(h))
-    barrier()
-    clk = clocks.stop()
-    check()
-    # the replayed K (same P as the recorded build) must be the streamed build's K; checked after
-    # the timed region, so the timed replays are the ones whose result is verified
-    Krep = np.zeros_like(K0_local)
-    lib.libgint_get_K(h, Krep.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
-    check()
-    replay_dev = max_over_ranks(float(np.abs(Krep - K0_local).max() / max(1e-300, np.abs(K0_local).max())))
-    if not replay_dev <= 1e-12:
-        raise RuntimeError(f"replayed K differs from the streamed build's K: rel max|dK| = {replay_dev:.3e}")
-    lib.libgint_get_stats(h, stats)
-    launches = (stats[4] - launches0) // max(1, args.steps)
-    tot_ms = max_over_ranks(float(np.sum(step_ms)))
-    ms_per_step = tot_ms / args.steps
-    value = total_shells / (ms_per_step / 1e3)
 
-    # 3) roofline: one profiled replay (kernels serialised on one stream) with event counters
-    lib.libgint_set_counters(h, 1)
-    kt = (ctypes.c_double * 2)()
-    lib.libgint_replay_profile(h, kt)
-    cnt = (ctypes.c_ulonglong * 1024)()
-    lib.libgint_get_counters(h, cnt)
-    lib.libgint_set_counters(h, 0)
+    def device_leg(thr, sampler):
+        """Record this rank's share (FP32 threshold thr, 0 = FP64), autotune the per-class kernels,
+        then time args.steps graph replays (CUDA events on the engine stream); one more replay with
+        the kernels serialised gives the per-family kernel times and the decision counters."""
+        set_fp32_threshold(thr)
+        try:
+            sess = Session(api, wl, max_mem_mb=args.max_mem_mb)
+            h = ctypes.c_void_p(sess.h)
+            lib.libgint_record(h, 1)
+            K_rec, ms_rec, _ = sess.build_K_subset(idx)
+            lib.libgint_record(h, 0)
+        finally:
+            set_fp32_threshold(0.0)
+        check(h)
+        lib.libgint_get_stats(h, stats)
+        st = list(stats)
+        tune = (ctypes.c_int * 512)()
+        if lib.libgint_autotune(h, tune):
+            check(h)
+        tune = np.array(tune).reshape(256, 2)
+        for _ in range(args.warmup):
+            lib.libgint_replay(h)
+        barrier()
+        lib.libgint_get_stats(h, stats)
+        launches0 = stats[4]
+        sampler.start()
+        step_ms = [lib.libgint_replay(h) for _ in range(args.steps)]
+        barrier()
+        clk = sampler.stop()
+        check(h)
+        K = np.zeros_like(K_rec)
+        lib.libgint_get_K(h, K.ctypes.data_as(D))
+        check(h)
+        # the replayed K (same P) must be the streamed build's, checked on the timed replays' result
+        dev = max_over_ranks(float(np.abs(K - K_rec).max() / max(1e-300, np.abs(K_rec).max())))
+        if not dev <= 1e-12:
+            raise RuntimeError(f"replayed K differs from the streamed build's K: rel max|dK| = {dev:.3e}")
+        lib.libgint_get_stats(h, stats)
+        launches = (stats[4] - launches0) // max(1, args.steps)
+        ms = max_over_ranks(float(np.sum(step_ms))) / args.steps
+        lib.libgint_set_counters(h, 1)
+        kt = (ctypes.c_double * 2)()
+        lib.libgint_replay_profile(h, kt)
+        cnt = (ctypes.c_ulonglong * 1024)()
+        lib.libgint_get_counters(h, cnt)
+        lib.libgint_set_counters(h, 0)
+        sess.close()
+        return {"K": sum_K(K), "ms": ms, "launches": int(launches), "kt": (kt[0], kt[1]), "cnt": np.array(cnt),
+                "clk": clk, "batches": int(st[3]), "fp32_shells": int(st[6]), "fp32_prims": int(st[7]),
+                "shells": int(st[0]), "prims": int(st[1]), "rec_bytes": int(st[5]), "replay_vs_stream": dev,
+                "tune": {"per_warp_prim_classes": int(tune[:, 0].sum()), "per_warp_group_classes": int(tune[:, 1].sum())}}
+
+    # 1) the all-FP64 path and 2) the mixed-precision path, both batched (one recording replayed as a
+    #    CUDA graph with autotuned per-class kernels)
+    fp64 = device_leg(0.0, ClockSampler(local))
+    mixed = device_leg(args.fp32_threshold, clocks)
+    value = total_shells / (mixed["ms"] / 1e3)
+    value_fp64 = total_shells / (fp64["ms"] / 1e3)
+    K64, Km = fp64["K"], mixed["K"]
+    mixed_dK = float(np.abs(Km - K64).max())
+    mixed_dEx = abs(wl.exchange_energy(Km) - wl.exchange_energy(K64)) if world == 1 or rank == 0 else None
+
+    # 3) roofline of the dominant kernel family of the mixed run (kernels serialised, CUDA events)
     fl = (ctypes.c_double * 8)()
     flops_prim = 0.0
+    cnt = mixed["cnt"]
     for c in range(256):
         ch, bo, vr = cnt[c * 4], cnt[c * 4 + 1], cnt[c * 4 + 2]
         if not (ch or bo or vr):
@@ -348,6 +485,7 @@ def run_ours(args, world, rank, local):
         flops_prim += ch * fl[0] + bo * fl[1] + vr * (fl[2] + fl[3])
     flops_group = group_flops(lib, wl) / world
     peak = lib.libgint_fp64_peak_tflops()
+    kt = mixed["kt"]
     fam = {
         "k_prim (Fm + VRR + image sum)": (flops_prim, kt[0]),
         "k_group (contraction + HRR + spherical + K update)": (flops_group, kt[1]),
@@ -359,71 +497,79 @@ def run_ours(args, world, rank, local):
     achieved = families[dom]["achieved_tflops"]
 
     if args.device_only:
-        sess.close()
         if rank == 0:
-            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "ms_per_step": ms_per_step,
-                              "device_only": True, "k_builds": args.warmup + args.steps + 2,
+            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "ms_per_step": mixed["ms"],
+                              "fp64": {"value": value_fp64, "ms_per_step": fp64["ms"]}, "device_only": True,
                               "workload": workload_desc(args, wl), "families": families,
-                              "replay_rel_max_dK_vs_stream": replay_dev}), flush=True)
+                              "mixed_max_dK_vs_fp64": mixed_dK}), flush=True)
         if pg:
             torch.distributed.destroy_process_group()
         return
 
-    # 4) CPU baseline (rank 0 at N=1): the oracle on a strided sub-sample, plus parity on it
+    # 4) CPU baseline (rank 0 at N=1): the oracle on a strided sub-sample, and parity there (FP64
+    #    engine element-wise against the oracle's magnitude K; mixed engine against the oracle)
     cpu = None
     parity = None
     if rank == 0 and world == 1:
-        from libgint_b200.workload import Api as _Api
         cidx, cshells, csample = oracle_sample(wl, args.cpu_seconds)
-        ora = Session(_Api(ORACLE_SO), wl)
+        ora = Session(Api(ORACLE_SO), wl)
         Ko, cms, _ = ora.build_K_subset(cidx)
         ora.close()
-        Ke, _, _ = sess.build_K_subset(cidx)
-        check()
-        # the sub-sample's K against the oracle, also element by element against the oracle's
-        # magnitude K (the scale of FP64 rounding error of each element; the basis is ill-conditioned)
-        ora = Session(_Api(ORACLE_SO), wl)
-        _Api(ORACLE_SO).symbol("oracle_set_absmode", None, [ctypes.c_void_p, ctypes.c_int])(ora.h, 1)
+        ora = Session(Api(ORACLE_SO), wl)
+        Api(ORACLE_SO).symbol("oracle_set_absmode", None, [ctypes.c_void_p, ctypes.c_int])(ora.h, 1)
         Kabs, _, _ = ora.build_K_subset(cidx)
         ora.close()
-        parity = {"rel_max_dK": float(np.abs(Ke - Ko).max() / max(1e-300, np.abs(Ko).max())),
-                  "max_dK_over_Kabs": float((np.abs(Ke - Ko) / np.maximum(Kabs, 1e-300)).max()),
+        Ks = {}
+        for name, thr in (("fp64", 0.0), ("mixed", args.fp32_threshold)):
+            set_fp32_threshold(thr)
+            try:
+                sess = Session(api, wl)
+                Ks[name], _, _ = sess.build_K_subset(cidx)
+                check(ctypes.c_void_p(sess.h))
+                sess.close()
+            finally:
+                set_fp32_threshold(0.0)
+        parity = {"sample": "the CPU baseline's sub-sample",
+                  "fp64_rel_max_dK": float(np.abs(Ks["fp64"] - Ko).max() / max(1e-300, np.abs(Ko).max())),
+                  "fp64_max_dK_over_Kabs": float((np.abs(Ks["fp64"] - Ko) / np.maximum(Kabs, 1e-300)).max()),
                   "Kabs_over_maxK": float(Kabs.max() / max(1e-300, np.abs(Ko).max())),
-                  "sample": "the CPU baseline's sub-sample"}
+                  "mixed_max_dK": float(np.abs(Ks["mixed"] - Ko).max()),
+                  "mixed_abs_dEx": abs(wl.exchange_energy(Ks["mixed"]) - wl.exchange_energy(Ko))}
         cpu = {"value": cshells / (cms / 1e3), "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                "sample": csample}
-    # the recording session's device batches and pinned queues are released before the
-    # end-to-end leg, which sets up its own handles
-    sess.close()
 
-    # 5) e2e through the C-ABI with host buffers, driven as CP2K's OpenMP team drives it
-    msess = MultiSession(api, wl, args.host_threads, max_mem_mb=args.host_mem_mb, team=True)
+    # 5) e2e through the C-ABI with host buffers, driven as CP2K's OpenMP team drives it, on the
+    #    mixed path (each thread passes its shell quartets' Schwarz bounds)
+    set_fp32_threshold(args.fp32_threshold)
+    try:
+        msess = MultiSession(api, wl, args.host_threads, max_mem_mb=args.host_mem_mb, team=True)
 
-    def h2d_total():
-        tot = 0
+        def h2d_total():
+            tot = 0
+            for hh in msess.hs:
+                lib.libgint_get_stats(ctypes.c_void_p(hh), stats)
+                tot += int(stats[5])
+            return tot
+
+        for _ in range(max(1, args.warmup - 1)):
+            msess.build_K(idx=idx)
+        barrier()
+        h2d0 = h2d_total()
+        e2e_ms = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            K, _, _ = msess.build_K(idx=idx)
+            K = sum_K(K)
+            e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        barrier()
         for hh in msess.hs:
-            lib.libgint_get_stats(ctypes.c_void_p(hh), stats)
-            tot += int(stats[5])
-        return tot
-
-    for _ in range(max(1, args.warmup - 1)):
-        msess.build_K(idx=idx)
-    barrier()
-    h2d0 = h2d_total()
-    e2e_ms = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        K, _, _ = msess.build_K(idx=idx)
-        K = sum_K(K)
-        e2e_ms.append((time.perf_counter() - t0) * 1e3)
-    barrier()
-    for hh in msess.hs:
-        check(ctypes.c_void_p(hh))
-    h2d = (h2d_total() - h2d0) // max(1, args.steps)
-    msess.close()
-    e2e_dev = float(np.abs(K - K0).max() / max(1e-300, np.abs(K0).max()))
-    e2e_tot = max_over_ranks(float(np.sum(e2e_ms)))
-    e2e_ms_step = e2e_tot / args.steps
+            check(ctypes.c_void_p(hh))
+        h2d = (h2d_total() - h2d0) // max(1, args.steps)
+        msess.close()
+    finally:
+        set_fp32_threshold(0.0)
+    e2e_dev = float(np.abs(K - Km).max())
+    e2e_ms_step = max_over_ranks(float(np.sum(e2e_ms))) / args.steps
     e2e_value = total_shells / (e2e_ms_step / 1e3)
     d2h = wl.info["flat_size"] * 8
 
@@ -431,38 +577,60 @@ def run_ours(args, world, rank, local):
     if rank == 0 and world == 1 and not args.no_reference_cuda:
         ref_cuda = reference_cuda_leg()
 
+    scf = None
+    if rank == 0 and world == 1 and args.scf_stride > 0:
+        scf = scf_leg(args, lib, api)
+    clusters = None
+    if rank == 0 and world == 1 and args.clusters_stride > 0:
+        clusters = clusters_leg(args, lib, api)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
-            "scaling": "weak" if world > 1 else "strong", "vs_baseline": None, "dtype": "f64",
+            "warmup": args.warmup, "ms_per_step": mixed["ms"], "higher_is_better": True,
+            "scaling": "weak" if world > 1 else "strong", "vs_baseline": None, "dtype": "f32/f64",
             "data": "synthetic",
             "config": {"workload": workload_desc(args, wl),
                        "shell_quartets": total_shells, "primitive_quartets": wl.info["n_prims"],
                        "set_quartets": nq, "contraction_rows": wl.info["n_qrtt"], "n_bf": wl.n_bf,
                        "images": wl.info["Ng"], "generation_s": t_gen,
-                       "l2": f"inputs larger than L2: {rec_bytes / 1e9:.2f} GB of quartet records "
+                       "fp32_threshold": args.fp32_threshold,
+                       "l2": f"inputs larger than L2: {mixed['rec_bytes'] / 1e9:.2f} GB of quartet records "
                              "are read from HBM per step (L2 is 126 MB)",
-                       "step": "one full K build over the sample's screened quartets (FP64)"},
+                       "step": "one full K build over the sample's screened quartets: mixed precision, one "
+                               "recording replayed as a CUDA graph with autotuned per-class kernels"},
+            "mixed": {"value": value, "ms_per_step": mixed["ms"], "gpu_launches": mixed["launches"],
+                      "batches": mixed["batches"], "fp32_shell_fraction": mixed["fp32_shells"] / max(1, mixed["shells"]),
+                      "fp32_primitive_fraction": mixed["fp32_prims"] / max(1, mixed["prims"]),
+                      "max_dK_vs_fp64_engine": mixed_dK, "abs_dEx_vs_fp64_engine": mixed_dEx,
+                      "autotune": mixed["tune"]},
+            "fp64": {"value": value_fp64, "ms_per_step": fp64["ms"], "gpu_launches": fp64["launches"],
+                     "batches": fp64["batches"], "autotune": fp64["tune"], "clocks": fp64["clk"]},
+            "mixed_speedup_vs_fp64": fp64["ms"] / mixed["ms"],
             "ms_per_scf_iter": e2e_ms_step,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms_step,
-                    "host_threads": args.host_threads, "caller": "OpenMP team, one handle per thread, shared K",
-                    "rel_max_dK_vs_recorded_build": e2e_dev},
-            "gpu_launches": int(launches),
+                    "host_threads": args.host_threads,
+                    "caller": "OpenMP team, one handle per thread, shared K, mixed precision",
+                    "max_dK_vs_device_mixed_build": e2e_dev},
+            "gpu_launches": mixed["launches"],
             "roofline": {"bound": "fp64", "kernel": dom, "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak if peak > 0 else None, "traffic": None,
                          "peak_source": "FP64 FMA rate measured on this GPU by libgint_fp64_peak_tflops "
                                         "(MEASURED_PEAKS.json has no FP64 figure)",
                          "families": families},
-            "clocks": clk,
-            "replay_rel_max_dK_vs_stream": replay_dev,
+            "clocks": mixed["clk"],
+            "replay_rel_max_dK_vs_stream": max(fp64["replay_vs_stream"], mixed["replay_vs_stream"]),
         }
         if cpu:
             line["cpu_baseline"] = cpu
-            line["parity_rel_max_dK_vs_oracle"] = parity
+            line["parity_vs_oracle"] = parity
         if ref_cuda is not None:
             line["reference_cuda"] = ref_cuda
+        if scf is not None:
+            line["scf_loop"] = scf
+        if clusters is not None:
+            line["batched_systems"] = clusters
         print(json.dumps(line), flush=True)
     if pg:
         torch.distributed.barrier()

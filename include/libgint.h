@@ -146,6 +146,12 @@ void libgint_record(void *handle, int on);
 /* recompute K from the recorded quartet list with the current P (after libgint_set_P), without
  * the add_* stream; K is then read with libgint_get_K. Returns the device time in ms. */
 double libgint_replay(void *handle);
+/* No counterpart in the reference. Incremental K update for SCF loops from the recorded quartet
+ * list: after libgint_set_P(dP) and libgint_set_K(K_previous), adds K(dP) to K (not zeroed), skipping
+ * every set quartet whose bound (libgint_add_shell_bound at recording time) scaled by
+ * max|dP| / max|P_recorded| over the P blocks it reads is below eps, and those dP does not touch.
+ * K_k = K_{k-1} + K(P_k - P_{k-1}) is then read with libgint_get_K. Returns the device time in ms. */
+double libgint_replay_incremental(void *handle, double eps);
 /* libgint_replay with the summed device time per kernel kind: kt[0] = Fm+VRR kernel,
  * kt[1] = contraction+HRR+spherical+K kernel (ms) */
 double libgint_replay_profile(void *handle, double *kt);

@@ -48,6 +48,7 @@ SIGNATURES = {
     "libgint_vrr_program": (ctypes.c_int, [ctypes.c_int] * 4 + [_V, ctypes.c_int, _I, ctypes.c_int]),
     "libgint_record": (None, [_V, ctypes.c_int]),
     "libgint_replay": (ctypes.c_double, [_V]),
+    "libgint_replay_incremental": (ctypes.c_double, [_V, ctypes.c_double]),
     "libgint_replay_profile": (ctypes.c_double, [_V, _D]),
     "libgint_replay_noalloc": (ctypes.c_int, [_V, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
     "libgint_add_set_quartets": (ctypes.c_int, [_V, ctypes.c_int] + [ctypes.c_void_p] * 11),

@@ -19,6 +19,7 @@
 #include <array>
 #include <atomic>
 #include <functional>
+#include <mutex>
 #include <chrono>
 #include <cmath>
 #include <cstdint>
@@ -193,6 +194,7 @@ struct gd_config {
    int setq_stride;     // > 1: keep the candidate set quartets (i,j,k,l) whose hash is setq_phase
    int setq_phase;      //      modulo setq_stride (a uniform sample of a workload too large to run whole)
    int threads;         // enumeration threads (0: all hardware threads); the result does not depend on it
+   int max_images;      // > 0: keep the max_images lattice vectors nearest the origin (origin first)
 };
 
 struct gd_info {
@@ -395,10 +397,19 @@ gd_workload *gd_create(const gd_config *cfg) {
       for (int q = 0; q < 3; q++) { w->cell_h[q * 3 + q] = Lb; w->cell_i[q * 3 + q] = 1.0 / Lb; }
       int k = cfg->n_img_1d / 2;
       w->neighs = {0.0, 0.0, 0.0};
+      std::vector<std::array<int, 3>> cells;
       for (int x = -k; x <= k; x++) for (int y = -k; y <= k; y++) for (int z = -k; z <= k; z++) {
          if (x == 0 && y == 0 && z == 0) continue;
-         w->neighs.insert(w->neighs.end(), {x * Lb, y * Lb, z * Lb});
+         cells.push_back({x, y, z});
       }
+      if (cfg->max_images > 0 && (int)cells.size() + 1 > cfg->max_images) {
+         // the nearest cells (a ball of images), ties kept in enumeration order
+         std::stable_sort(cells.begin(), cells.end(), [](const std::array<int, 3> &a, const std::array<int, 3> &b) {
+            return a[0] * a[0] + a[1] * a[1] + a[2] * a[2] < b[0] * b[0] + b[1] * b[1] + b[2] * b[2];
+         });
+         cells.resize(cfg->max_images - 1);
+      }
+      for (const auto &c : cells) w->neighs.insert(w->neighs.end(), {c[0] * Lb, c[1] * Lb, c[2] * Lb});
    } else {
       // a cell far larger than the system makes the minimum-image wrap the identity
       for (int q = 0; q < 3; q++) { w->cell_h[q * 3 + q] = 1024.0; w->cell_i[q * 3 + q] = 1.0 / 1024.0; }
@@ -420,13 +431,23 @@ gd_workload *gd_create(const gd_config *cfg) {
       nn = std::sqrt(nn); for (int i = 0; i < n; i++) v[i] /= nn;
    }
    w->P.assign((size_t)n * n, 0.0);
-   for (int c = 0; c < no; c++) {
-      const double *v = &C[(size_t)c * n];
-      for (int col = 0; col < n; col++) {
-         double vc = 2.0 * v[col];
-         double *Pc = &w->P[(size_t)col * n];
-         for (int r = 0; r < n; r++) Pc[r] += vc * v[r];
-      }
+   {
+      // columns of P in parallel; each column sums the orbitals in the same order as a serial loop
+      const int nth = cfg->threads > 0 ? cfg->threads : std::max(1, (int)std::thread::hardware_concurrency());
+      std::atomic<int> next{0};
+      std::vector<std::thread> th;
+      for (int t = 0; t < nth; t++)
+         th.emplace_back([&]() {
+            for (int col; (col = next.fetch_add(1)) < n;) {
+               double *Pc = &w->P[(size_t)col * n];
+               for (int c = 0; c < no; c++) {
+                  const double *v = &C[(size_t)c * n];
+                  const double vc = 2.0 * v[col];
+                  for (int r = 0; r < n; r++) Pc[r] += vc * v[r];
+               }
+            }
+         });
+      for (auto &x : th) x.join();
    }
    // ---- packed block layout: blocks (X,Y) with X >= Y, column-major, ld = functions of X
    const int S = (int)w->sets.size();
@@ -621,8 +642,19 @@ gd_workload *gd_create(const gd_config *cfg) {
    // ---- C0
    w->nder = 12;
    const int ld = (w->nder + 1) * 105;
-   w->C0.assign((size_t)TCG_NPATCH * ld, 0.0);
-   gd_tcg_table(w->nder, w->C0.data());
+   {
+      // the fit depends only on nder: made once per process and copied into every workload
+      static std::mutex mu;
+      static std::vector<double> fitted;
+      static int fitted_nder = -1;
+      std::lock_guard<std::mutex> lock(mu);
+      if (fitted_nder != w->nder) {
+         fitted.assign((size_t)TCG_NPATCH * ld, 0.0);
+         gd_tcg_table(w->nder, fitted.data());
+         fitted_nder = w->nder;
+      }
+      w->C0 = fitted;
+   }
    return w;
 }
 
@@ -696,6 +728,17 @@ long gd_get_shell_prims(const gd_workload *w, long h, uint32_t *out) {
    const Shell &sh = w->shells[h];
    std::memcpy(out, &w->prims[sh.prm_begin], sizeof(uint32_t) * (sh.prm_end - sh.prm_begin));
    return (long)(sh.prm_end - sh.prm_begin);
+}
+
+// a dense symmetric n_bf x n_bf matrix (column-major) in the packed set-pair block layout of P/K
+void gd_pack(const gd_workload *w, const double *dense, double *flat) {
+   const int S = (int)w->sets.size(), n = w->n_bf;
+   auto nbf_of = [&](int x) { const SetDef &d = w->defs[w->sets[x].def]; return (2 * d.l + 1) * d.nl; };
+   for (int x = 0; x < S; x++) for (int y = 0; y <= x; y++) {
+      const int nx = nbf_of(x), ny = nbf_of(y), bx = w->sets[x].bf_off, by = w->sets[y].bf_off;
+      double *blk = flat + w->blkoff[(size_t)x * S + y];
+      for (int c = 0; c < ny; c++) for (int r = 0; r < nx; r++) blk[(size_t)c * nx + r] = dense[(size_t)(by + c) * n + bx + r];
+   }
 }
 
 // the screening estimate of every shell quartet, in the workload's shell order
@@ -803,9 +846,9 @@ static double build_K_impl(const gd_workload *w, gd_api *a, void *h, const doubl
 static int g_reverse_prims = 0;
 static int g_bulk = 0;        // stream through libgint_add_set_quartets when the library has it
 void gd_set_bulk(int on) { g_bulk = on; }
-// mixed precision: every K build sets this threshold (libgint_set_fp32_threshold) and passes each
-// shell quartet's bound (libgint_add_shell_bound) before its add_shell, where the library has them;
-// 0 = FP64 (no bounds passed)
+// mixed precision: every K build sets this threshold (libgint_set_fp32_threshold, 0 = FP64) where
+// the library has it; each shell quartet's bound goes before its add_shell (libgint_add_shell_bound)
+// wherever the library takes one (it also drives incremental replays' screening)
 static double g_fp32_thr = 0.0;
 void gd_set_fp32_threshold(double thr) { g_fp32_thr = thr; }
 static long g_only_shell = -1;   // replay only this shell (index within its set quartet), -1: all
@@ -906,51 +949,57 @@ static void stream_bulk(const gd_workload *w, gd_api *a, void *h, long q0, long 
    }
 }
 
+// The per-call add_* stream of one set quartet: add_prm* add_shell per image pair (with its bound
+// when bounds is set), add_qrt, add_qrtt per contraction row, add_set. The workload's set indices are
+// shifted by set_off and its P/K offsets by flat_off (several systems in one handle).
+static void stream_setq(const gd_workload *w, gd_api *a, void *h, const SetQ &q, int set_off, uint32_t flat_off,
+                        bool bounds) {
+   const int S = (int)w->sets.size();
+   const Set *s4[4] = {&w->sets[q.i], &w->sets[q.j], &w->sets[q.k], &w->sets[q.l]};
+   const SetDef *d4[4] = {&w->defs[s4[0]->def], &w->defs[s4[1]->def], &w->defs[s4[2]->def], &w->defs[s4[3]->def]};
+   for (uint32_t hs = q.shell_begin; hs < q.shell_end; hs++) {
+      if (g_only_shell >= 0 && (long)(hs - q.shell_begin) != g_only_shell) continue;
+      const Shell &sh = w->shells[hs];
+      for (uint32_t pp = sh.prm_begin; pp < sh.prm_end; pp++) {
+         const uint32_t p = g_reverse_prims ? sh.prm_end - 1 - (pp - sh.prm_begin) : pp;
+         uint32_t c = w->prims[p];
+         a->prm(h, c >> 24, (c >> 16) & 255, (c >> 8) & 255, c & 255);
+      }
+      if (bounds) a->bound(h, (double)sh.bound);
+      a->shell(h, q.i + set_off, q.j + set_off, q.k + set_off, q.l + set_off, sh.n1, sh.n2);
+   }
+   const int la = d4[0]->l, lb = d4[1]->l, lc = d4[2]->l, ld = d4[3]->l;
+   a->qrt(h, la, lb, lc, ld, d4[0]->nl, d4[1]->nl, d4[2]->nl, d4[3]->nl);
+   // K/P addressing in the packed block layout: the pair (x,y) lands in block (max, min);
+   // T selects the transposed walk when x < y. ld = functions of the block's row set (< 256).
+   auto addr = [&](int sx, int sy, int inx, int iny, unsigned &off, int &ldv, bool &T) {
+      qrtt_addr(w, S, sx, sy, inx, iny, off, ldv, T);
+      off += flat_off;
+   };
+   for (int ia = 0; ia < d4[0]->nl; ia++) for (int ib = 0; ib < d4[1]->nl; ib++)
+   for (int ic = 0; ic < d4[2]->nl; ic++) for (int id = 0; id < d4[3]->nl; id++) {
+      unsigned oac, oad, obc, obd; int lac, lad, lbc, lbd; bool Tac, Tad, Tbc, Tbd;
+      addr(q.i, q.k, ia, ic, oac, lac, Tac);
+      addr(q.i, q.l, ia, id, oad, lad, Tad);
+      addr(q.j, q.k, ib, ic, obc, lbc, Tbc);
+      addr(q.j, q.l, ib, id, obd, lbd, Tbd);
+      a->qrtt(h, (double)q.fac, la, lb, lc, ld, ia, ib, ic, id, lac, lad, lbc, lbd, oac, oad, obc, obd,
+              Tac, Tad, Tbc, Tbd);
+   }
+   a->addset(h);
+}
+
 static double build_K_impl(const gd_workload *w, gd_api *a, void *h, const double *P, double *K,
                            long q0, long q1, const long *idx, double *times, bool bulk) {
    using clk = std::chrono::steady_clock;
-   const int S = (int)w->sets.size();
    if (!idx && (q1 < 0 || q1 > (long)w->setq.size())) q1 = (long)w->setq.size();
    auto t0 = clk::now();
    if (a->fp32thr) a->fp32thr(h, g_fp32_thr);
-   const bool bounds = g_fp32_thr > 0.0 && a->bound;
+   const bool bounds = a->bound != nullptr;
    a->setP(h, const_cast<double *>(P ? P : w->Pflat.data()), (int)w->flat_size);
    auto t1 = clk::now();
    if (bulk && a->bulk) stream_bulk(w, a, h, q0, q1, idx);
-   else for (long iq0 = q0; iq0 < q1; iq0++) {
-      const SetQ &q = w->setq[idx ? idx[iq0] : iq0];
-      const Set *s4[4] = {&w->sets[q.i], &w->sets[q.j], &w->sets[q.k], &w->sets[q.l]};
-      const SetDef *d4[4] = {&w->defs[s4[0]->def], &w->defs[s4[1]->def], &w->defs[s4[2]->def], &w->defs[s4[3]->def]};
-      for (uint32_t hs = q.shell_begin; hs < q.shell_end; hs++) {
-         if (g_only_shell >= 0 && (long)(hs - q.shell_begin) != g_only_shell) continue;
-         const Shell &sh = w->shells[hs];
-         for (uint32_t pp = sh.prm_begin; pp < sh.prm_end; pp++) {
-            const uint32_t p = g_reverse_prims ? sh.prm_end - 1 - (pp - sh.prm_begin) : pp;
-            uint32_t c = w->prims[p];
-            a->prm(h, c >> 24, (c >> 16) & 255, (c >> 8) & 255, c & 255);
-         }
-         if (bounds) a->bound(h, (double)sh.bound);
-         a->shell(h, q.i, q.j, q.k, q.l, sh.n1, sh.n2);
-      }
-      const int la = d4[0]->l, lb = d4[1]->l, lc = d4[2]->l, ld = d4[3]->l;
-      a->qrt(h, la, lb, lc, ld, d4[0]->nl, d4[1]->nl, d4[2]->nl, d4[3]->nl);
-      // K/P addressing in the packed block layout: the pair (x,y) lands in block (max, min);
-      // T selects the transposed walk when x < y. ld = functions of the block's row set (< 256).
-      auto addr = [&](int sx, int sy, int inx, int iny, unsigned &off, int &ld, bool &T) {
-         qrtt_addr(w, S, sx, sy, inx, iny, off, ld, T);
-      };
-      for (int ia = 0; ia < d4[0]->nl; ia++) for (int ib = 0; ib < d4[1]->nl; ib++)
-      for (int ic = 0; ic < d4[2]->nl; ic++) for (int id = 0; id < d4[3]->nl; id++) {
-         unsigned oac, oad, obc, obd; int lac, lad, lbc, lbd; bool Tac, Tad, Tbc, Tbd;
-         addr(q.i, q.k, ia, ic, oac, lac, Tac);
-         addr(q.i, q.l, ia, id, oad, lad, Tad);
-         addr(q.j, q.k, ib, ic, obc, lbc, Tbc);
-         addr(q.j, q.l, ib, id, obd, lbd, Tbd);
-         a->qrtt(h, (double)q.fac, la, lb, lc, ld, ia, ib, ic, id, lac, lad, lbc, lbd, oac, oad, obc, obd,
-                 Tac, Tad, Tbc, Tbd);
-      }
-      a->addset(h);
-   }
+   else for (long iq0 = q0; iq0 < q1; iq0++) stream_setq(w, a, h, w->setq[idx ? idx[iq0] : iq0], 0, 0, bounds);
    auto t2 = clk::now();
    a->getK(h, K);
    auto t3 = clk::now();
@@ -1038,6 +1087,63 @@ double gd_build_K_team(const gd_workload *w, gd_api *a, void **handles, int nh, 
       times[4] = 0.0;
    }
    return std::chrono::duration<double, std::milli>(t1 - t0).count();
+}
+
+// ----- several independent systems in one handle -----------------------------------------
+// The systems' sets are registered one after another (system k's set s is set_off[k] + s) and
+// their packed P/K arrays are concatenated (system k's at flat_off[k]); every set quartet lies
+// within one system, so the engine sees one class-sorted quartet list over all of them. All
+// systems share the potential, the cell and the image list of the first (non-periodic clusters).
+void *gd_setup_multi(const gd_workload *const *ws, int n, gd_api *a, int max_mem_mb) {
+   void *h = a->create();
+   a->init(h);
+   gd_workload *w0 = const_cast<gd_workload *>(ws[0]);
+   a->pot(h, w0->rc_bohr, w0->C0.data(), (w0->nder + 1) * 105, (int)w0->C0.size());
+   a->hf(h, 1.0);
+   a->maxmem(h, max_mem_mb);
+   a->cell(h, w0->cfg.periodic != 0, w0->cell_h, w0->cell_i);
+   a->neighs(h, w0->neighs.data(), w0->Ng);
+   int off = 0;
+   for (int k = 0; k < n; k++) {
+      gd_workload *w = const_cast<gd_workload *>(ws[k]);
+      for (size_t s = 0; s < w->sets.size(); s++) {
+         const SetDef &d = w->defs[w->sets[s].def];
+         a->atom(h, off + (int)s, w->sets[s].R, const_cast<double *>(d.Z.data()), d.np);
+         a->atomL(h, off + (int)s, d.l, d.nl, const_cast<double *>(d.Kraw.data()));
+      }
+      off += (int)w->sets.size();
+   }
+   return h;
+}
+
+// One K build over every set quartet of the n systems in one handle: set_P with the concatenated
+// packed P, the add_* stream system after system, get_K into K (the concatenated packed K, sum of
+// the systems' flat sizes). Returns wall ms; times as gd_build_K.
+double gd_build_K_multi(const gd_workload *const *ws, int n, gd_api *a, void *h, double *K, double *times) {
+   using clk = std::chrono::steady_clock;
+   size_t tot = 0;
+   for (int k = 0; k < n; k++) tot += ws[k]->flat_size;
+   std::vector<double> P(tot);
+   size_t fo = 0;
+   for (int k = 0; k < n; k++) { std::memcpy(P.data() + fo, ws[k]->Pflat.data(), ws[k]->flat_size * 8); fo += ws[k]->flat_size; }
+   auto t0 = clk::now();
+   if (a->fp32thr) a->fp32thr(h, g_fp32_thr);
+   const bool bounds = a->bound != nullptr;
+   a->setP(h, P.data(), (int)tot);
+   auto t1 = clk::now();
+   int so = 0;
+   fo = 0;
+   for (int k = 0; k < n; k++) {
+      for (const SetQ &q : ws[k]->setq) stream_setq(ws[k], a, h, q, so, (uint32_t)fo, bounds);
+      so += (int)ws[k]->sets.size();
+      fo += ws[k]->flat_size;
+   }
+   auto t2 = clk::now();
+   a->getK(h, K);
+   auto t3 = clk::now();
+   auto ms = [](clk::time_point x, clk::time_point y) { return std::chrono::duration<double, std::milli>(y - x).count(); };
+   if (times) { times[0] = ms(t0, t1); times[1] = ms(t1, t2); times[2] = ms(t2, t3); }
+   return ms(t0, t3);
 }
 
 void gd_teardown(gd_api *a, void *h) { if (a->destroy) a->destroy(h); }

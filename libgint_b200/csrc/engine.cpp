@@ -165,6 +165,7 @@ struct OpenGroup {
    uint8_t nl[4];
    bool have_qrt;
    int nq;
+   double bound;     // largest bound of the group's shell quartets (HUGE_VAL once one has none)
 };
 
 // Growable array in pinned host memory (pageable if no device is present), so that a batch is
@@ -306,12 +307,14 @@ struct Handle {
    int cur = 0;
    // record / replay of the device-resident quartet list
    struct RecSeg { int c; size_t o_prm, o_ps, o_sh, o_g, o_q, o_rg, ac_off; uint32_t nprm, nshell, ngroup, nqrtt; };
-   struct RecBatch { DBuf rec; std::vector<RecSeg> segs; size_t ac_doubles = 0; };
+   // per recorded batch: its records, its class segments, and (gbuf) each segment's per-group
+   // largest |P| of the recording (float) and incremental-replay flags (byte) at g_pmax[i], g_flag[i]
+   struct RecBatch { DBuf rec, gbuf; std::vector<RecSeg> segs; std::vector<size_t> g_pmax, g_flag; size_t ac_doubles = 0; };
    bool recording = false;
    std::vector<RecBatch> recs;
    long long rec_gen = 0;           // bumped whenever the recording changes
    // the replay captured as a CUDA graph, and what it was captured with
-   struct GraphKey { DevCtx ctx; long long rec_gen; void *ac, *gscr; size_t half; };
+   struct GraphKey { DevCtx ctx; long long rec_gen; void *ac, *gscr; size_t half; double eps; };
    cudaGraphExec_t graph_exec = nullptr;
    GraphKey graph_key;
    long long graph_launches = 0;
@@ -389,6 +392,7 @@ static inline OpenGroup *open_group(Handle *h, int c) {
    g.nl[0] = g.nl[1] = g.nl[2] = g.nl[3] = 0;
    g.have_qrt = false;
    g.nq = 0;
+   g.bound = 0.0;
    return &g;
 }
 
@@ -802,10 +806,13 @@ static void set_K_impl(Handle *h, int nspin, const double *Ka, const double *Kb,
 // kt == nullptr the segments spread over the worker streams (forked from and joined back to the
 // handle's stream), otherwise they run in order on the handle's stream with an event before and
 // after each kernel (kev, kcl: per-kernel timing). ac is the replay AC buffer's half size.
+// eps >= 0: an incremental replay (K is not zeroed; each segment's groups are screened against
+// eps first, see k_group_screen, and the screened ones skipped).
 static bool enqueue_replay(Handle *h, const DevCtx &ctx, size_t ac, std::vector<cudaEvent_t> *kev,
-                           std::vector<int> *kcl, long long *nlaunch) {
-   for (int sp = 0; sp < h->nspin; sp++)
-      if (!ck(h, cudaMemsetAsync(h->team->K[sp].p, 0, h->FP_size * 8, h->stream), "K zero")) return false;
+                           std::vector<int> *kcl, long long *nlaunch, double eps = -1.0) {
+   if (eps < 0.0)
+      for (int sp = 0; sp < h->nspin; sp++)
+         if (!ck(h, cudaMemsetAsync(h->team->K[sp].p, 0, h->FP_size * 8, h->stream), "K zero")) return false;
    auto kmark = [&]() {
       if (!kev) return;
       cudaEvent_t e; cudaEventCreate(&e); cudaEventRecord(e, h->stream); kev->push_back(e);
@@ -821,7 +828,8 @@ static bool enqueue_replay(Handle *h, const DevCtx &ctx, size_t ac, std::vector<
          for (int w = 0; w < kWorkStreams; w++)
             for (int w2 = 0; w2 < kWorkStreams; w2++)
                if (!ck(h, cudaStreamWaitEvent(h->work[w], h->batch_ev[bi & 1][w2], 0), "stream wait")) return false;
-      for (auto &g : rb.segs) {
+      for (size_t si = 0; si < rb.segs.size(); si++) {
+         const auto &g = rb.segs[si];
          BatchArgs bt;
          std::memset(&bt, 0, sizeof(bt));
          bt.cls = g.c & 255;
@@ -841,6 +849,14 @@ static bool enqueue_replay(Handle *h, const DevCtx &ctx, size_t ac, std::vector<
          int a_, b_;
          const ClassPlan &hp = h->plans[g.c & 255];
          cudaStream_t st = spread ? worker_for(h, nseg++, group_global_scratch(hp, &a_, &b_) != 0) : h->stream;
+         if (eps >= 0.0) {
+            char *gb = (char *)rb.gbuf.p;
+            uint8_t *flags = (uint8_t *)(gb + rb.g_flag[si]);
+            if (!ck(h, launch_group_screen(ctx, bt, (float *)(gb + rb.g_pmax[si]), flags, eps, 1, st), "screen launch"))
+               return false;
+            bt.gflags = flags;
+            *nlaunch += 1;
+         }
          kmark();
          if (kcl) kcl->push_back(g.c & 255);
          if (!ck(h, launch_prim(ctx, bt, hp, st), "k_prim launch")) return false;
@@ -892,9 +908,12 @@ static bool prepare_replay(Handle *h, size_t *half) {
    return true;
 }
 
-static double replay_impl(Handle *h, double *kt, double *kcls = nullptr) {
+static double replay_impl(Handle *h, double *kt, double *kcls = nullptr, double eps = -1.0) {
    size_t ac = 0;
    if (!prepare_replay(h, &ac)) return -1.0;
+   if (eps >= 0.0)
+      for (auto &rb : h->recs)
+         if (!rb.gbuf.p) { set_error(h, 4, "libgint_replay_incremental: the recording has no group screening data"); return -1.0; }
    DevCtx ctx = make_ctx(h);
    cudaEvent_t e0, e1;
    cudaEventCreate(&e0); cudaEventCreate(&e1);
@@ -903,7 +922,7 @@ static double replay_impl(Handle *h, double *kt, double *kcls = nullptr) {
       std::vector<cudaEvent_t> kev;
       std::vector<int> kcl;
       ck(h, cudaEventRecord(e0, h->stream), "event");
-      enqueue_replay(h, ctx, ac, &kev, &kcl, &h->n_launch);
+      enqueue_replay(h, ctx, ac, &kev, &kcl, &h->n_launch, eps);
       ck(h, cudaEventRecord(e1, h->stream), "event");
       ck(h, cudaEventSynchronize(e1), "replay");
       kt[0] = kt[1] = 0.0;
@@ -921,14 +940,14 @@ static double replay_impl(Handle *h, double *kt, double *kcls = nullptr) {
       std::memset(&key, 0, sizeof(key));
       std::memcpy(&key.ctx, &ctx, sizeof(ctx));
       key.rec_gen = h->rec_gen;
-      key.ac = h->rec_ac.p; key.gscr = h->rec_gscr.p; key.half = ac;
+      key.ac = h->rec_ac.p; key.gscr = h->rec_gscr.p; key.half = ac; key.eps = eps;
       if (!h->graph_exec || std::memcmp(&key, &h->graph_key, sizeof(key)) != 0) {
          drop_graph(h);
          cudaGraph_t graph = nullptr;
          long long n = 0;
          bool ok = ck(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "graph capture");
          if (ok) {
-            ok = enqueue_replay(h, ctx, ac, nullptr, nullptr, &n);
+            ok = enqueue_replay(h, ctx, ac, nullptr, nullptr, &n, eps);
             const cudaError_t ec = cudaStreamEndCapture(h->stream, &graph);
             ok = ok && ck(h, ec, "graph capture");
          }
@@ -948,6 +967,38 @@ static double replay_impl(Handle *h, double *kt, double *kcls = nullptr) {
    cudaEventElapsedTime(&ms, e0, e1);
    cudaEventDestroy(e0); cudaEventDestroy(e1);
    return h->err ? -1.0 : (double)ms;
+}
+
+// After a recording: per recorded segment, each group's largest |P| over the blocks its rows read,
+// with the recording's P (for the screening of incremental replays, libgint_replay_incremental).
+static void record_group_pmax(Handle *h) {
+   if (h->err || h->recs.empty() || !h->team || !h->team->ok) return;
+   use_device(h);
+   DevCtx ctx = make_ctx(h);
+   for (auto &rb : h->recs) {
+      if (rb.gbuf.p) continue;
+      size_t off = 0;
+      rb.g_pmax.clear(); rb.g_flag.clear();
+      for (auto &g : rb.segs) {
+         rb.g_pmax.push_back(off); off = al16(off + (size_t)g.ngroup * 4);
+         rb.g_flag.push_back(off); off = al16(off + (size_t)g.ngroup);
+      }
+      if (!ensure(h, rb.gbuf, std::max<size_t>(off, 256), "recorded screening data")) return;
+      char *base = (char *)rb.rec.p;
+      for (size_t si = 0; si < rb.segs.size(); si++) {
+         const auto &g = rb.segs[si];
+         BatchArgs bt;
+         std::memset(&bt, 0, sizeof(bt));
+         bt.cls = g.c & 255;
+         bt.groups = (const GroupRec *)(base + g.o_g);
+         bt.qrtts = (const QrttRec *)(base + g.o_q);
+         bt.ngroup = g.ngroup; bt.nqrtt = g.nqrtt;
+         if (!ck(h, launch_group_screen(ctx, bt, (float *)((char *)rb.gbuf.p + rb.g_pmax[si]), nullptr, 0.0, 0, h->stream),
+                 "screen launch"))
+            return;
+      }
+   }
+   ck(h, cudaStreamSynchronize(h->stream), "recorded screening data");
 }
 
 // The autotuner: for every class of the recording, the primitive kernels (generated per-lane VRR,
@@ -1205,6 +1256,7 @@ void libgint_add_shell(void *hh, int i, int j, int k, int l, int n1, int n2) {
       h->next_bound = HUGE_VAL;
       OpenGroup *og = open_group(h, cl);
       if (!og) { set_error(h, 2, "libgint_add_shell: too many l-combinations in one set quartet"); h->prm_tmp.clear(); return; }
+      og->bound = std::max(og->bound, bound);
       ClassQ &Q = h->q[cl];
       ShellRec sr;
       sr.ent[0] = (uint32_t)fa.ent; sr.ent[1] = (uint32_t)fb.ent; sr.ent[2] = (uint32_t)fc.ent; sr.ent[3] = (uint32_t)fd.ent;
@@ -1233,6 +1285,7 @@ static void add_shell_general(Handle *h, const int idx[4], int n1, int n2) {
       const int cl = shell_qclass(h, cls_of(S4[0]->l[a], S4[1]->l[b], S4[2]->l[c], S4[3]->l[d]));
       OpenGroup *og = open_group(h, cl);
       if (!og) { set_error(h, 2, "libgint_add_shell: too many l-combinations in one set quartet"); break; }
+      og->bound = std::max(og->bound, h->next_bound);
       ClassQ &Q = h->q[cl];
       ShellRec sr;
       const int li[4] = {a, b, c, d};
@@ -1323,16 +1376,22 @@ constexpr size_t kChunkWork = 4096;
 // stay for the primitive kernel) and its own copy of the rows. Contraction, HRR, spherical
 // transform and K update are linear, so the chunks' K updates add up to the group's.
 static void commit_group(Handle *h, ClassQ &Q, int qcls, uint32_t shell0, uint32_t qrtt0, size_t prm0,
-                         const uint8_t nl[4], int nrows) {
+                         const uint8_t nl[4], int nrows, double bound) {
    const uint32_t nshell = (uint32_t)Q.shells.size() - shell0;
    const size_t nprm = Q.prm.size() - prm0;
    const size_t S = (size_t)h->S_of[qcls & 255];
    const size_t cap = std::max<size_t>(32, kChunkWork / std::max<size_t>(S, 1));
    size_t recs = nprm * 8 + (size_t)nshell * sizeof(ShellRec);
+   // every record of the set quartet's shells names its group (the primitive kernel reads the
+   // first group's flag on an incremental replay)
+   const uint32_t first_group = (uint32_t)Q.groups.size();
+   for (uint32_t si = shell0; si < shell0 + nshell; si++) Q.shells.data()[si].group = first_group;
    auto push_group = [&](uint32_t sh_off, uint32_t nsh, uint32_t q_off) {
       GroupRec g;
       g.shell_off = sh_off; g.nshell = nsh; g.qrtt_off = q_off;
       for (int q = 0; q < 4; q++) g.nl[q] = nl[q];
+      g.bound = bound < 3.0e38 ? (float)bound : INFINITY;
+      for (uint32_t si = sh_off; si < sh_off + nsh; si++) Q.shells.data()[si].group = (uint32_t)Q.groups.size();
       Q.groups.push_back(g);
       recs += sizeof(GroupRec) + (size_t)nrows * sizeof(QrttRec);
    };
@@ -1394,7 +1453,7 @@ void libgint_add_set(void *hh) {
          Q.qrtts.resize(og.qrtt_off);
          continue;
       }
-      commit_group(h, Q, og.cls, og.shell_off, og.qrtt_off, og.prm_off, og.nl, nrows);
+      commit_group(h, Q, og.cls, og.shell_off, og.qrtt_off, og.prm_off, og.nl, nrows, og.bound);
    }
    h->nopen = 0;
    const size_t budget = slot_budget_bytes(h);
@@ -1479,7 +1538,7 @@ int libgint_add_set_quartets(void *hh, int n, const int *sets, const int *shell_
             if (nshell > 0) {
                uint8_t nl4[4];
                for (int u = 0; u < 4; u++) nl4[u] = (uint8_t)r[4 + u];
-               commit_group(h, Q, cl, shell0, qrtt0, prm0, nl4, nrow);
+               commit_group(h, Q, cl, shell0, qrtt0, prm0, nl4, nrow, HUGE_VAL);
             } else {
                Q.qrtts.resize(qrtt0);   // nothing to compute: the group rolls back, as in add_set
             }
@@ -1548,16 +1607,26 @@ void libgint_record(void *hh, int on) {
    if (on) {
       drain(h);
       drop_graph(h);
-      for (auto &rb : h->recs) release(rb.rec);
+      for (auto &rb : h->recs) { release(rb.rec); release(rb.gbuf); }
       h->recs.clear();
    } else {
       flush(h);
+      record_group_pmax(h);
    }
    h->recording = on != 0;
    h->rec_gen++;
 }
 
 double libgint_replay(void *hh) { return replay_impl((Handle *)hh, nullptr); }
+
+// Incremental K update from the recorded quartet list (no counterpart in the reference): with the
+// current P = dP (libgint_set_P) and K = the previous K (libgint_set_K), adds K(dP) to K without
+// zeroing it, skipping every set quartet whose recorded bound scaled by max|dP| / max|P_recorded|
+// over the P blocks it reads is below eps (and the ones dP does not touch). The SCF loop's
+// K_k = K_{k-1} + K(P_k - P_{k-1}). Returns the device time in ms, like libgint_replay.
+double libgint_replay_incremental(void *hh, double eps) {
+   return replay_impl((Handle *)hh, nullptr, nullptr, eps < 0.0 ? 0.0 : eps);
+}
 
 // The per-class kernel choice (no counterpart in the reference): libgint_autotune times both
 // primitive kernels and both group kernels of every class on the recorded quartet list (after
@@ -1812,7 +1881,7 @@ void libgint_destroy_handle(void *hh) {
       if (s.ev) cudaEventDestroy(s.ev);
       if (s.ev_copy) cudaEventDestroy(s.ev_copy);
    }
-   for (auto &rb : h->recs) release(rb.rec);
+   for (auto &rb : h->recs) { release(rb.rec); release(rb.gbuf); }
    release(h->rec_ac); release(h->rec_gscr); release(h->d_cnt);
    DBuf *bufs[] = {&h->d_pool, &h->d_ents, &h->d_neighs, &h->d_C0, &h->d_C0f, &h->d_lut, &h->d_bw, &h->d_ft, &h->d_vops,
                    &h->d_plans, &h->d_err};

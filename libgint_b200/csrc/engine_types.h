@@ -25,7 +25,8 @@ struct ShellRec {
    uint32_t prm_off;    // first primitive quartet of this shell in the batch
    uint32_t nprm;
    uint16_t n1, n2;
-   uint32_t group;      // owning group (set quartet, l-combination)
+   uint32_t group;      // owning group in the class segment (for the primitive kernel's records: the
+                        // set quartet's first group)
 };
 
 // All image pairs of one set quartet for one class, and its contraction rows.
@@ -33,6 +34,7 @@ struct GroupRec {
    uint32_t shell_off, nshell;
    uint32_t qrtt_off;   // first KS record; the group owns nla*nlb*nlc*nld consecutive rows
    uint8_t nl[4];
+   float bound;         // largest Schwarz bound of its shell quartets given by the caller (+inf: none)
 };
 
 // One row of the exchange update (reference KS record, src/define.h:172-179, decoded).

@@ -55,7 +55,7 @@ __global__ void __launch_bounds__(128, Group3Shape<LA, LB, LC, LD>::MINB) k_grou
    for (uint32_t blk = blockIdx.x * wpb + (threadIdx.x >> 5); blk < nblk; blk += gridDim.x * wpb) {
       const uint32_t q0 = blk << 5, q = q0 + lane;
       const uint32_t gi = row_group_warp(bt, q0, lane);
-      if (q >= bt.nqrtt) continue;
+      if (q >= bt.nqrtt || (bt.gflags && !__ldg(bt.gflags + gi))) continue;   // screened (incremental)
       const GroupRec Gr = bt.groups[gi];
       const int nl1 = Gr.nl[1], nl2 = Gr.nl[2], nl3 = Gr.nl[3];
       const int r = (int)(q - Gr.qrtt_off);

@@ -143,6 +143,7 @@ __global__ void __launch_bounds__(256) k_prim(DevCtx ctx, BatchArgs bt, int team
    for (uint32_t p = blockIdx.x * nteam + team; p < bt.nprm; p += gridDim.x * nteam) {
       PrimGeo g;
       prim_geometry(ctx, bt.shells[bt.prm_shell[p]], bt.prm[p], g);
+      kill_if_screened(bt, bt.shells[bt.prm_shell[p]], g);
 
       for (int j = lane; j < S; j += TS) acc[j] = 0.0;
       double s00 = 0.0;
@@ -155,7 +156,7 @@ __global__ void __launch_bounds__(256) k_prim(DevCtx ctx, BatchArgs bt, int team
          const int n3 = n0 + lane;
          bool surv = false;
          double *myfm = fmx + lane * (L + 1);
-         if (n3 < ctx.Ng) {
+         if (n3 < ctx.Ng && !(g.upper < 0.0)) {
             const double T = image_T(ctx, g, n3);
             const int br = fm_eval(ctx, L, g.R, T, g.Kfac, myfm);
             c_cheb += (br == 1); c_boys += (br == 2);
@@ -276,6 +277,7 @@ __global__ void __launch_bounds__(256) k_prim2(DevCtx ctx, BatchArgs bt, int cp,
          const uint32_t p = p0 + lane;
          PrimGeo g;
          prim_geometry(ctx, bt.shells[bt.prm_shell[p]], bt.prm[p], g);
+         kill_if_screened(bt, bt.shells[bt.prm_shell[p]], g);
          geo[lane] = g;
          s00[lane] = 0.0;
       }
@@ -406,7 +408,7 @@ __global__ void __launch_bounds__(256) k_prim2(DevCtx ctx, BatchArgs bt, int cp,
             const int p = pi / Ng, n3 = pi - p * Ng;
             const PrimGeo &g = geo[p];
             T = image_T(ctx, g, n3);
-            pass = !(T > trunc_upper(g.R));
+            pass = !(T > g.upper);   // g.upper = trunc_upper(g.R), or -1 for a screened primitive
          }
          const unsigned bal = __ballot_sync(0xffffffffu, pass);
          if (pass) {
@@ -678,7 +680,9 @@ __global__ void __launch_bounds__(256) k_group(DevCtx ctx, BatchArgs bt, int war
    const int Hws = max(pl->H, 2 * pl->Nc);
    const uint2 *hrec = ctx.gprog + ctx.gprog[bt.cls].x;
    for (uint32_t q = gwarp; q < bt.nqrtt; q += gridDim.x * nwarp) {
-      const GroupRec G = bt.groups[row_group_one(bt, q, lane)];
+      const uint32_t gi = row_group_one(bt, q, lane);
+      if (bt.gflags && !__ldg(bt.gflags + gi)) continue;   // screened on an incremental replay
+      const GroupRec G = bt.groups[gi];
       group_body<32, 1>(ctx, bt, pl, G, q, wbase, wbase + Hws, lane, hrec, kpw);
    }
 }
@@ -698,7 +702,7 @@ __global__ void __launch_bounds__(256) k_group_lane(DevCtx ctx, BatchArgs bt, in
    for (uint32_t blk = blockIdx.x * nwarp + warp; blk < nblk; blk += gridDim.x * nwarp) {
       const uint32_t q0 = blk << 5, q = q0 + lane;
       const uint32_t gi = row_group_warp(bt, q0, lane);
-      if (q >= bt.nqrtt) continue;
+      if (q >= bt.nqrtt || (bt.gflags && !__ldg(bt.gflags + gi))) continue;
       const GroupRec G = bt.groups[gi];
       group_body<1, 32>(ctx, bt, pl, G, q, wbase, wbase + Hws * 32, 0, hrec, nullptr);
    }
@@ -947,6 +951,53 @@ cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan
       const size_t smem = plan_bytes + (size_t)warps * kGroupKpDoubles * 8;
       k_group<<<grid, warps * 32, smem, st>>>(ctx, bt, (int)wd, 1);
    }
+   return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------------
+// k_group_screen: incremental replays. One thread per group: the largest |P| over the P elements
+// its rows' K updates read (blocks ac: nsa x nsc, ad: nsa x nsd, bc: nsb x nsc, bd: nsb x nsd, with
+// each row's offsets, leading dimensions and transposition flags). Mode 0 stores it (the recording's
+// P); mode 1 (P = dP) keeps the group unless dP vanishes on its blocks or its bound scaled by
+// max|dP| / max|P_recorded| is below eps.
+// ---------------------------------------------------------------------------------------
+__global__ void k_group_screen(DevCtx ctx, BatchArgs bt, float *pmax, uint8_t *flags, double eps, int mode) {
+   const int la = bt.cls >> 6, lb = (bt.cls >> 4) & 3, lc = (bt.cls >> 2) & 3, ld = bt.cls & 3;
+   const int ns[4] = {2 * la + 1, 2 * lb + 1, 2 * lc + 1, 2 * ld + 1};
+   // block u of a row: rows of centre bra[u], columns of centre ket[u] (ac, ad, bc, bd)
+   const int bra[4] = {0, 0, 1, 1}, ket[4] = {2, 3, 2, 3};
+   const double *Pm = ctx.P[0];
+   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < bt.ngroup; g += gridDim.x * blockDim.x) {
+      const GroupRec G = bt.groups[g];
+      const int nrows = G.nl[0] * G.nl[1] * G.nl[2] * G.nl[3];
+      double m = 0.0;
+      for (int r = 0; r < nrows; r++) {
+         const QrttRec k = bt.qrtts[G.qrtt_off + r];
+         for (int u = 0; u < 4; u++) {
+            const bool T = (k.T >> u) & 1;
+            for (int i = 0; i < ns[bra[u]]; i++)
+               for (int j = 0; j < ns[ket[u]]; j++) {
+                  const size_t I = (size_t)k.off[u] + (T ? i * k.ld[u] + j : j * k.ld[u] + i);
+                  if (I < ctx.FP_size) m = fmax(m, fabs(__ldg(Pm + I)));
+               }
+         }
+      }
+      if (mode == 0) {
+         pmax[g] = (float)m;
+      } else {
+         const double b = (double)G.bound;
+         const bool skip = m == 0.0 || (isfinite(b) && b * m < eps * (double)pmax[g]);
+         flags[g] = skip ? 0 : 1;
+      }
+   }
+}
+
+cudaError_t launch_group_screen(const DevCtx &ctx, const BatchArgs &bt, float *pmax, uint8_t *flags, double eps,
+                                int mode, cudaStream_t st) {
+   if (bt.ngroup == 0) return cudaSuccess;
+   const int threads = 128;
+   const long blocks = std::max(1L, std::min(((long)bt.ngroup + threads - 1) / threads, 148L * 16));
+   k_group_screen<<<(unsigned)blocks, threads, 0, st>>>(ctx, bt, pmax, flags, eps, mode);
    return cudaGetLastError();
 }
 

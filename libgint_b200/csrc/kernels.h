@@ -56,6 +56,7 @@ struct BatchArgs {
    uint32_t nprm, nshell, ngroup;
    uint32_t nqrtt;            // contraction rows (the group kernels' work items), in group order
    const uint32_t *rowgrp;    // group of row 32 k, k < (nqrtt + 31) / 32
+   const uint8_t *gflags;     // incremental replay: 0 = skip the group (its primitives and rows); null = all run
    double *AC;                // [nprm][S] image-summed VRR targets (floats in the first half for fp32)
    int fp32;                  // 1: the segment's shell quartets run in FP32 (Fm, VRR, contraction, HRR)
    double *gscratch;          // HRR workspace in global memory for the largest classes
@@ -72,6 +73,11 @@ cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan
 size_t group_global_scratch(const ClassPlan &hp, int *grid, int *warps);
 constexpr int kGroupKpDoubles = 32;   // per-warp shared buffer of contraction coefficients in k_group
 int prim_team_size(const ClassPlan &hp);
+// Incremental replay screening (k_group_screen): mode 0 writes each group's largest |P| over the P
+// blocks its rows read into pmax (the recording's P); mode 1 sets flags[g] = 0 for the groups whose
+// bound * max|dP| / pmax is below eps (current P = dP) and 1 for the others.
+cudaError_t launch_group_screen(const DevCtx &ctx, const BatchArgs &bt, float *pmax, uint8_t *flags, double eps,
+                                int mode, cudaStream_t st);
 // whether k_prim3 (generated VRR) covers class cls (prim3.cu)
 bool prim_has_generated(int cls);
 // classes with an FP32 path (generated VRR and HRR code): la + lb + lc + ld <= 3

@@ -119,7 +119,9 @@ k_prim3(DevCtx ctx, BatchArgs bt) {
       const int np = (int)min((uint32_t)CP, bt.nprm - p0);
       if (lane < np) {
          PrimGeo g;
-         prim_geometry(ctx, bt.shells[bt.prm_shell[p0 + lane]], bt.prm[p0 + lane], g);
+         const ShellRec sh = bt.shells[bt.prm_shell[p0 + lane]];
+         prim_geometry(ctx, sh, bt.prm[p0 + lane], g);
+         kill_if_screened(bt, sh, g);
          geo[lane] = g;
       }
       for (int j = lane; j < CP * S; j += 32) acc[j] = R(0);

@@ -164,6 +164,12 @@ static __device__ __forceinline__ void prim_geometry(const DevCtx &ctx, const Sh
    g.i2 = i2 == 128 ? 127 : i2;
 }
 
+// Incremental replays skip the primitives of screened groups: their truncation bound is set below
+// every T, so no image of theirs is evaluated and their targets stay zero.
+static __device__ __forceinline__ void kill_if_screened(const BatchArgs &bt, const ShellRec &sh, PrimGeo &g) {
+   if (bt.gflags && !__ldg(bt.gflags + sh.group)) g.upper = -1.0;
+}
+
 // T = rho |P - Q - neighs[n3]|^2 (reference src/compute_Fm.cpp:204-210)
 static __device__ __forceinline__ double image_T(const DevCtx &ctx, const PrimGeo &g, int n3) {
    const double PQ0 = rsub(g.D[0], __ldg(ctx.neighs + n3 * 3 + 0));

@@ -8,6 +8,7 @@ the libgint_* entry points. The named configurations follow the benchmark defini
   periodic_l2   32 molecules, 9.86 A cubic cell, 27 images, l<=2, 128 occupied orbitals
   periodic_l2_small  12 molecules at the same density (7.1 A cell), for kernel profiling
   periodic_l3   64 molecules, 12.4 A cell, 125 images, l<=3 basis with general contraction
+  periodic_l3_scf  128 molecules, 15.6 A cell, the 256 image cells nearest the origin, l<=3 basis
 """
 import ctypes
 import os
@@ -25,7 +26,7 @@ class GdConfig(ctypes.Structure):
                 ("rc_ang", ctypes.c_double), ("eps_schwarz", ctypes.c_double),
                 ("seed", ctypes.c_uint64), ("full_enum", ctypes.c_int), ("max_prm", ctypes.c_int),
                 ("max_ncontr", ctypes.c_int), ("setq_stride", ctypes.c_int), ("setq_phase", ctypes.c_int),
-                ("threads", ctypes.c_int)]
+                ("threads", ctypes.c_int), ("max_images", ctypes.c_int)]
 
 
 class GdInfo(ctypes.Structure):
@@ -41,6 +42,7 @@ CONFIGS = {
     "periodic_l2": dict(n_mol=32, box_ang=9.86, periodic=1, n_img_1d=3, basis=2, n_occ=128),
     "periodic_l2_small": dict(n_mol=12, box_ang=7.1, periodic=1, n_img_1d=3, basis=2, n_occ=48),
     "periodic_l3": dict(n_mol=64, box_ang=12.4, periodic=1, n_img_1d=5, basis=3, n_occ=256),
+    "periodic_l3_scf": dict(n_mol=128, box_ang=15.6, periodic=1, n_img_1d=7, basis=3, n_occ=512, max_images=256),
 }
 
 _D = ctypes.POINTER(ctypes.c_double)
@@ -84,6 +86,13 @@ def driver():
         lib.gd_mt_split.restype = None
         lib.gd_mt_split.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_long), ctypes.c_long, ctypes.c_int,
                                     ctypes.POINTER(ctypes.c_long)]
+        lib.gd_pack.restype = None
+        lib.gd_pack.argtypes = [ctypes.c_void_p, _D, _D]
+        lib.gd_setup_multi.restype = ctypes.c_void_p
+        lib.gd_setup_multi.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
+        lib.gd_build_K_multi.restype = ctypes.c_double
+        lib.gd_build_K_multi.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_void_p,
+                                         ctypes.c_void_p, _D, _D]
         lib.gd_set_fp32_threshold.restype = None
         lib.gd_set_fp32_threshold.argtypes = [ctypes.c_double]
         lib.gd_get_shell_bounds.restype = None
@@ -109,15 +118,16 @@ class Workload:
     """A generated system plus its screened add_* call stream."""
 
     def __init__(self, name=None, seed=0, eps_schwarz=1e-11, rc_ang=6.0, full_enum=False,
-                 max_prm=16, max_ncontr=4, setq_stride=1, setq_phase=0, threads=0, **overrides):
+                 max_prm=16, max_ncontr=4, setq_stride=1, setq_phase=0, threads=0, max_images=0, **overrides):
         params = dict(CONFIGS[name]) if name else {}
         params.update(overrides)
+        max_images = params.pop("max_images", max_images)
         cfg = GdConfig(n_mol=params["n_mol"], box_ang=params["box_ang"],
                        periodic=params["periodic"], n_img_1d=params["n_img_1d"],
                        basis=params["basis"], n_occ=params["n_occ"], rc_ang=rc_ang,
                        eps_schwarz=eps_schwarz, seed=seed, full_enum=int(full_enum),
                        max_prm=max_prm, max_ncontr=max_ncontr, setq_stride=setq_stride,
-                       setq_phase=setq_phase, threads=threads)
+                       setq_phase=setq_phase, threads=threads, max_images=max_images)
         self.name = name
         self.params = params
         self._w = driver().gd_create(ctypes.byref(cfg))
@@ -145,6 +155,13 @@ class Workload:
         P = np.empty(self.info["flat_size"])
         driver().gd_get_Pflat(self._w, _dp(P))
         return P
+
+    def pack(self, dense):
+        """A dense symmetric n_bf x n_bf matrix in the packed set-pair block layout of P/K."""
+        d = np.ascontiguousarray(np.asarray(dense, dtype=np.float64).reshape(self.n_bf, self.n_bf).T)
+        flat = np.empty(self.info["flat_size"])
+        driver().gd_pack(self._w, _dp(d), _dp(flat))
+        return flat
 
     def unpack_K(self, K_flat):
         """Dense symmetric exchange matrix from the packed K returned by get_K."""
@@ -281,6 +298,50 @@ class MultiSession:
             if h:
                 driver().gd_teardown(self.api._a, h)
         self.hs = []
+
+
+class SystemBatch:
+    """Several independent systems driven through ONE handle: their sets are registered one after
+    another and their packed P/K arrays concatenated, so the engine batches all their quartets into
+    one class-sorted list (and one recorded replay). Every set quartet lies within one system."""
+
+    def __init__(self, workloads):
+        self.wls = list(workloads)
+        self._arr = (ctypes.c_void_p * len(self.wls))(*[w._w for w in self.wls])
+        self.flat = np.array([w.info["flat_size"] for w in self.wls], dtype=np.int64)
+        self.offsets = np.concatenate([[0], np.cumsum(self.flat)])
+        self.info = {k: sum(w.info[k] for w in self.wls) for k in ("n_setq", "n_shells", "n_prims", "n_qrtt", "n_sets")}
+
+    def setup(self, api, max_mem_mb=7000):
+        return driver().gd_setup_multi(self._arr, len(self.wls), api._a, max_mem_mb)
+
+    def build_K(self, api, h):
+        """One K build of every system through handle h: (K of each system, wall ms)."""
+        K = np.zeros(int(self.offsets[-1]))
+        t = np.zeros(3)
+        ms = driver().gd_build_K_multi(self._arr, len(self.wls), api._a, h, _dp(K), _dp(t))
+        return self.split(K), ms
+
+    def split(self, K):
+        return [K[self.offsets[i]:self.offsets[i + 1]] for i in range(len(self.wls))]
+
+    def exchange_energies(self, Ks):
+        return np.array([w.exchange_energy(k) for w, k in zip(self.wls, Ks)])
+
+
+def cluster_batch(n_systems=96, seed=0, min_mol=2, max_mol=24, setq_stride=1, threads=0):
+    """Independent non-periodic water clusters of min_mol..max_mol molecules (uniform, one seed per
+    system), alternating the l <= 2 and l <= 3 bases, at the 4-molecule system's density (12 A box
+    for 4 molecules), each with 5 occupied orbitals per molecule."""
+    rng = np.random.default_rng(seed)
+    sizes = rng.integers(min_mol, max_mol + 1, size=n_systems)
+    wls = []
+    for k, m in enumerate(sizes):
+        basis = 3 if k % 2 else 2
+        wls.append(Workload(None, seed=seed * 100003 + k + 1, setq_stride=setq_stride, threads=threads,
+                            n_mol=int(m), box_ang=12.0 * (m / 4.0) ** (1.0 / 3.0), periodic=0, n_img_1d=1,
+                            basis=basis, n_occ=5 * int(m)))
+    return SystemBatch(wls)
 
 
 def set_fp32_threshold(thr):
