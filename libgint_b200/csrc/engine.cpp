@@ -278,6 +278,7 @@ struct Handle {
    bool basis_dirty = true, ent_dirty = true;
    // device-resident data
    DBuf d_pool, d_ents, d_neighs, d_C0, d_C0f, d_lut, d_bw, d_ft, d_plans, d_err, d_vops;
+   DBuf d_tmax;                     // incremental replays: tile maxima of |dP|
    std::vector<VOp> vops;           // precompiled VRR instructions of all classes
    std::shared_ptr<Team> team;      // device P and K (shared by the handles of an OpenMP team)
    int nspin = 0;
@@ -810,9 +811,14 @@ static void set_K_impl(Handle *h, int nspin, const double *Ka, const double *Kb,
 // eps first, see k_group_screen, and the screened ones skipped).
 static bool enqueue_replay(Handle *h, const DevCtx &ctx, size_t ac, std::vector<cudaEvent_t> *kev,
                            std::vector<int> *kcl, long long *nlaunch, double eps = -1.0) {
-   if (eps < 0.0)
+   if (eps < 0.0) {
       for (int sp = 0; sp < h->nspin; sp++)
          if (!ck(h, cudaMemsetAsync(h->team->K[sp].p, 0, h->FP_size * 8, h->stream), "K zero")) return false;
+   } else {
+      // tile maxima of |dP| for the groups' screening (before the fork: every worker needs them)
+      if (!ck(h, launch_tile_max(ctx.P[0], h->FP_size, (float *)h->d_tmax.p, h->stream), "tile max launch")) return false;
+      *nlaunch += 1;
+   }
    auto kmark = [&]() {
       if (!kev) return;
       cudaEvent_t e; cudaEventCreate(&e); cudaEventRecord(e, h->stream); kev->push_back(e);
@@ -852,7 +858,8 @@ static bool enqueue_replay(Handle *h, const DevCtx &ctx, size_t ac, std::vector<
          if (eps >= 0.0) {
             char *gb = (char *)rb.gbuf.p;
             uint8_t *flags = (uint8_t *)(gb + rb.g_flag[si]);
-            if (!ck(h, launch_group_screen(ctx, bt, (float *)(gb + rb.g_pmax[si]), flags, eps, 1, st), "screen launch"))
+            if (!ck(h, launch_group_screen(ctx, bt, (float *)(gb + rb.g_pmax[si]), flags, eps, 1,
+                                           (const float *)h->d_tmax.p, st), "screen launch"))
                return false;
             bt.gflags = flags;
             *nlaunch += 1;
@@ -911,9 +918,11 @@ static bool prepare_replay(Handle *h, size_t *half) {
 static double replay_impl(Handle *h, double *kt, double *kcls = nullptr, double eps = -1.0) {
    size_t ac = 0;
    if (!prepare_replay(h, &ac)) return -1.0;
-   if (eps >= 0.0)
+   if (eps >= 0.0) {
       for (auto &rb : h->recs)
          if (!rb.gbuf.p) { set_error(h, 4, "libgint_replay_incremental: the recording has no group screening data"); return -1.0; }
+      if (!ensure(h, h->d_tmax, std::max<size_t>(tile_max_count(h->FP_size) * 4, 256), "tile maxima")) return -1.0;
+   }
    DevCtx ctx = make_ctx(h);
    cudaEvent_t e0, e1;
    cudaEventCreate(&e0); cudaEventCreate(&e1);
@@ -993,7 +1002,8 @@ static void record_group_pmax(Handle *h) {
          bt.groups = (const GroupRec *)(base + g.o_g);
          bt.qrtts = (const QrttRec *)(base + g.o_q);
          bt.ngroup = g.ngroup; bt.nqrtt = g.nqrtt;
-         if (!ck(h, launch_group_screen(ctx, bt, (float *)((char *)rb.gbuf.p + rb.g_pmax[si]), nullptr, 0.0, 0, h->stream),
+         if (!ck(h, launch_group_screen(ctx, bt, (float *)((char *)rb.gbuf.p + rb.g_pmax[si]), nullptr, 0.0, 0, nullptr,
+                                        h->stream),
                  "screen launch"))
             return;
       }
@@ -1612,6 +1622,16 @@ void libgint_record(void *hh, int on) {
    } else {
       flush(h);
       record_group_pmax(h);
+      // the streaming slots' buffers are not needed to replay; release them, so that a recording's
+      // replays hold the recorded batches and the replay buffers only (a streamed build allocates
+      // them again)
+      if (!h->err && ck(h, cudaStreamSynchronize(h->stream), "record")) {
+         for (Slot &sl : h->slots) {
+            if (sl.busy) { ck(h, cudaEventSynchronize(sl.ev), "slot wait"); sl.busy = false; }
+            sl.copy_busy = false;
+            release(sl.rec); release(sl.ac); release(sl.gscr);
+         }
+      }
    }
    h->recording = on != 0;
    h->rec_gen++;
@@ -1883,7 +1903,7 @@ void libgint_destroy_handle(void *hh) {
    }
    for (auto &rb : h->recs) { release(rb.rec); release(rb.gbuf); }
    release(h->rec_ac); release(h->rec_gscr); release(h->d_cnt);
-   DBuf *bufs[] = {&h->d_pool, &h->d_ents, &h->d_neighs, &h->d_C0, &h->d_C0f, &h->d_lut, &h->d_bw, &h->d_ft, &h->d_vops,
+   DBuf *bufs[] = {&h->d_pool, &h->d_ents, &h->d_neighs, &h->d_C0, &h->d_C0f, &h->d_lut, &h->d_bw, &h->d_ft, &h->d_vops, &h->d_tmax,
                    &h->d_plans, &h->d_err};
    for (DBuf *b : bufs) release(*b);
    h->team.reset();

@@ -955,13 +955,32 @@ cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan
 }
 
 // ---------------------------------------------------------------------------------------
-// k_group_screen: incremental replays. One thread per group: the largest |P| over the P elements
-// its rows' K updates read (blocks ac: nsa x nsc, ad: nsa x nsd, bc: nsb x nsc, bd: nsb x nsd, with
-// each row's offsets, leading dimensions and transposition flags). Mode 0 stores it (the recording's
-// P); mode 1 (P = dP) keeps the group unless dP vanishes on its blocks or its bound scaled by
-// max|dP| / max|P_recorded| is below eps.
+// Incremental replays. k_group_screen, one thread per group:
+//  mode 0 (after a recording): the exact largest |P| over the P elements its rows' K updates read
+//    (blocks ac: nsa x nsc, ad: nsa x nsd, bc: nsb x nsc, bd: nsb x nsd, with each row's offsets,
+//    leading dimensions and transposition flags), stored in pmax;
+//  mode 1 (P = dP): an upper bound of max|dP| over the same elements, from the maxima of 32-element
+//    tiles of |dP| (k_tile_max) over the span of offsets each block's rows cover, and the group kept
+//    unless that bound is zero or its bound scaled by it / pmax is below eps. The span bound never
+//    underestimates, so no group that the exact test keeps is skipped.
 // ---------------------------------------------------------------------------------------
-__global__ void k_group_screen(DevCtx ctx, BatchArgs bt, float *pmax, uint8_t *flags, double eps, int mode) {
+constexpr int kScreenTile = 32;
+
+__global__ void k_tile_max(const double *__restrict__ P, size_t n, float *__restrict__ tmax) {
+   const size_t ntile = (n + kScreenTile - 1) / kScreenTile;
+   const int lane = threadIdx.x & 31;
+   for (size_t t = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) / 32; t < ntile;
+        t += (size_t)gridDim.x * blockDim.x / 32) {
+      const size_t i = t * kScreenTile + lane;
+      double m = i < n ? fabs(__ldg(P + i)) : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+      if (lane == 0) tmax[t] = (float)(m * (1.0 + 1e-6));   // rounded up: stays an upper bound
+   }
+}
+
+__global__ void k_group_screen(DevCtx ctx, BatchArgs bt, float *pmax, uint8_t *flags, double eps, int mode,
+                               const float *tmax) {
    const int la = bt.cls >> 6, lb = (bt.cls >> 4) & 3, lc = (bt.cls >> 2) & 3, ld = bt.cls & 3;
    const int ns[4] = {2 * la + 1, 2 * lb + 1, 2 * lc + 1, 2 * ld + 1};
    // block u of a row: rows of centre bra[u], columns of centre ket[u] (ac, ad, bc, bd)
@@ -971,33 +990,56 @@ __global__ void k_group_screen(DevCtx ctx, BatchArgs bt, float *pmax, uint8_t *f
       const GroupRec G = bt.groups[g];
       const int nrows = G.nl[0] * G.nl[1] * G.nl[2] * G.nl[3];
       double m = 0.0;
-      for (int r = 0; r < nrows; r++) {
-         const QrttRec k = bt.qrtts[G.qrtt_off + r];
-         for (int u = 0; u < 4; u++) {
-            const bool T = (k.T >> u) & 1;
-            for (int i = 0; i < ns[bra[u]]; i++)
-               for (int j = 0; j < ns[ket[u]]; j++) {
-                  const size_t I = (size_t)k.off[u] + (T ? i * k.ld[u] + j : j * k.ld[u] + i);
-                  if (I < ctx.FP_size) m = fmax(m, fabs(__ldg(Pm + I)));
-               }
-         }
-      }
       if (mode == 0) {
+         for (int r = 0; r < nrows; r++) {
+            const QrttRec k = bt.qrtts[G.qrtt_off + r];
+            for (int u = 0; u < 4; u++) {
+               const bool T = (k.T >> u) & 1;
+               for (int i = 0; i < ns[bra[u]]; i++)
+                  for (int j = 0; j < ns[ket[u]]; j++) {
+                     const size_t I = (size_t)k.off[u] + (T ? i * k.ld[u] + j : j * k.ld[u] + i);
+                     if (I < ctx.FP_size) m = fmax(m, fabs(__ldg(Pm + I)));
+                  }
+            }
+         }
          pmax[g] = (float)m;
-      } else {
-         const double b = (double)G.bound;
-         const bool skip = m == 0.0 || (isfinite(b) && b * m < eps * (double)pmax[g]);
-         flags[g] = skip ? 0 : 1;
+         continue;
       }
+      for (int u = 0; u < 4; u++) {
+         size_t lo = ~(size_t)0, hi = 0;
+         for (int r = 0; r < nrows; r++) {
+            const QrttRec k = bt.qrtts[G.qrtt_off + r];
+            const bool T = (k.T >> u) & 1;
+            const int nr = ns[bra[u]], nc = ns[ket[u]];
+            const size_t a = k.off[u];
+            const size_t e = a + (T ? (size_t)(nr - 1) * k.ld[u] + nc : (size_t)(nc - 1) * k.ld[u] + nr);
+            lo = min(lo, a);
+            hi = max(hi, e);
+         }
+         hi = min(hi, ctx.FP_size);
+         for (size_t t = lo / kScreenTile; lo < hi && t * kScreenTile < hi; t++) m = fmax(m, (double)__ldg(tmax + t));
+      }
+      const double b = (double)G.bound;
+      const bool skip = m == 0.0 || (isfinite(b) && b * m < eps * (double)pmax[g]);
+      flags[g] = skip ? 0 : 1;
    }
 }
 
+cudaError_t launch_tile_max(const double *P, size_t n, float *tmax, cudaStream_t st) {
+   const size_t ntile = (n + kScreenTile - 1) / kScreenTile;
+   const long blocks = std::max(1L, std::min((long)((ntile * 32 + 255) / 256), 148L * 32));
+   k_tile_max<<<(unsigned)blocks, 256, 0, st>>>(P, n, tmax);
+   return cudaGetLastError();
+}
+
+size_t tile_max_count(size_t n) { return (n + kScreenTile - 1) / kScreenTile; }
+
 cudaError_t launch_group_screen(const DevCtx &ctx, const BatchArgs &bt, float *pmax, uint8_t *flags, double eps,
-                                int mode, cudaStream_t st) {
+                                int mode, const float *tmax, cudaStream_t st) {
    if (bt.ngroup == 0) return cudaSuccess;
    const int threads = 128;
    const long blocks = std::max(1L, std::min(((long)bt.ngroup + threads - 1) / threads, 148L * 16));
-   k_group_screen<<<(unsigned)blocks, threads, 0, st>>>(ctx, bt, pmax, flags, eps, mode);
+   k_group_screen<<<(unsigned)blocks, threads, 0, st>>>(ctx, bt, pmax, flags, eps, mode, tmax);
    return cudaGetLastError();
 }
 

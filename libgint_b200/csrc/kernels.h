@@ -75,9 +75,13 @@ constexpr int kGroupKpDoubles = 32;   // per-warp shared buffer of contraction c
 int prim_team_size(const ClassPlan &hp);
 // Incremental replay screening (k_group_screen): mode 0 writes each group's largest |P| over the P
 // blocks its rows read into pmax (the recording's P); mode 1 sets flags[g] = 0 for the groups whose
-// bound * max|dP| / pmax is below eps (current P = dP) and 1 for the others.
+// bound * max|dP| / pmax is below eps (current P = dP; max|dP| bounded from the tile maxima tmax of
+// launch_tile_max) and 1 for the others.
 cudaError_t launch_group_screen(const DevCtx &ctx, const BatchArgs &bt, float *pmax, uint8_t *flags, double eps,
-                                int mode, cudaStream_t st);
+                                int mode, const float *tmax, cudaStream_t st);
+// maxima of |P| over consecutive tiles of 32 elements (an upper bound, rounded up), tile_max_count(n)
+cudaError_t launch_tile_max(const double *P, size_t n, float *tmax, cudaStream_t st);
+size_t tile_max_count(size_t n);
 // whether k_prim3 (generated VRR) covers class cls (prim3.cu)
 bool prim_has_generated(int cls);
 // classes with an FP32 path (generated VRR and HRR code): la + lb + lc + ld <= 3
