@@ -75,9 +75,9 @@ __global__ void __launch_bounds__(128, Group3Shape<LA, LB, LC, LD>::MINB) k_grou
 #pragma unroll
          for (int j = 0; j < S; j++) T[j] = R(0);
          const R *AC = reinterpret_cast<const R *>(bt.AC);
-         // contraction over the primitives (reference src/compute_ECO.cpp:131-212); two per
-         // iteration so that the next one's loads overlap this one's FMAs
-#pragma unroll 2
+         // contraction over the primitives (reference src/compute_ECO.cpp:131-212); four per
+         // iteration so that the next ones' loads overlap this one's FMAs
+#pragma unroll 4
          for (uint32_t ip = 0; ip < sh.nprm; ip++) {
             const uint32_t code = __ldg(bt.prm + sh.prm_off + ip);
             const R kp = (R)__ldg(Ka + (code >> 24)) * (R)__ldg(Kb + ((code >> 16) & 255)) *

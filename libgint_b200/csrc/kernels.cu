@@ -665,7 +665,7 @@ static __device__ __forceinline__ void load_plan(const ClassPlan *src_plan, doub
 }
 
 // one warp per contraction row
-__global__ void __launch_bounds__(256) k_group(DevCtx ctx, BatchArgs bt, int warp_doubles, int use_global) {
+__global__ void __launch_bounds__(256, 3) k_group(DevCtx ctx, BatchArgs bt, int warp_doubles, int use_global) {
    extern __shared__ __align__(16) double smem[];
    const ClassPlan *pl = reinterpret_cast<const ClassPlan *>(smem);
    load_plan(bt.plan, smem);
