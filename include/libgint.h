@@ -160,10 +160,12 @@ double libgint_replay_profile_classes(void *handle, double *kt, double *kcls);
 /* No counterpart in the reference. Per-class kernel choice: after libgint_record and libgint_set_P,
  * libgint_autotune times, for every class of the recorded quartet list, the primitive kernel with
  * generated per-lane VRR against the per-warp interpreted one, and the group kernel with one lane
- * per contraction row (generated HRR) against one warp per row (interpreted HRR), and keeps the
- * faster of each for every following launch; out[2c], out[2c+1] (c = la*64+lb*16+lc*4+ld; 512 ints,
- * may be NULL) receive the choices (0 = per-lane, 1 = per-warp). libgint_set_tuning installs such a
- * table, libgint_get_tuning reads it. Returns 0 or the error code. */
+ * per contraction row (generated HRR; classes with la+lb+lc+ld <= 3) or one block per row
+ * (interpreted HRR; the other classes, where the workspace fits a block's shared memory) against one
+ * warp per row (interpreted HRR), and keeps the faster of each for every following launch;
+ * out[2c], out[2c+1] (c = la*64+lb*16+lc*4+ld; 512 ints, may be NULL) receive the choices
+ * (0 = per-lane or per-block, 1 = per-warp). libgint_set_tuning installs such a table,
+ * libgint_get_tuning reads it. Returns 0 or the error code. */
 int libgint_autotune(void *handle, int *out);
 void libgint_set_tuning(void *handle, const int *in);
 void libgint_get_tuning(void *handle, int *out);

@@ -1047,10 +1047,9 @@ static int autotune_impl(Handle *h, int *out) {
          bt.nprm = g.nprm; bt.nshell = g.nshell; bt.ngroup = g.ngroup; bt.nqrtt = g.nqrtt;
          bt.AC = ac_half + g.ac_off;
          bt.gscratch = (double *)h->rec_gscr.p;
-         const int cl[4] = {c >> 6, (c >> 4) & 3, (c >> 2) & 3, c & 3};
          seen[c] = true;
          alt_p[c] = prim_has_generated(c);
-         alt_g[c] = class_has_fp32(cl[0], cl[1], cl[2], cl[3]);
+         alt_g[c] = true;   // variant 0: k_group3, or k_group_block where it applies; variant 1: k_group
          ck(h, cudaEventRecord(ev[0], h->stream), "event");
          bt.prim_variant = 1;
          ck(h, launch_prim(ctx, bt, hp, h->stream), "k_prim launch");
@@ -1659,9 +1658,8 @@ void libgint_set_tuning(void *hh, const int *in) {
    Handle *h = (Handle *)hh;
    drop_graph(h);
    for (int c = 0; c < 256; c++) {
-      const int cl[4] = {c >> 6, (c >> 4) & 3, (c >> 2) & 3, c & 3};
       h->tune_prim[c] = in[2 * c] ? 1 : 0;
-      h->tune_group[c] = (in[2 * c + 1] && class_has_fp32(cl[0], cl[1], cl[2], cl[3])) ? 1 : 0;
+      h->tune_group[c] = in[2 * c + 1] ? 1 : 0;
    }
 }
 

@@ -126,8 +126,15 @@ template <int LA, int LB, int LC, int LD>
 cudaError_t launch_one(const DevCtx &ctx, const BatchArgs &bt, cudaStream_t st) {
    const int threads = 128;
    const long blocks = std::max(1L, std::min(((long)bt.nqrtt + threads - 1) / threads, 148L * 16));
-   if (bt.fp32) k_group3<LA, LB, LC, LD, float><<<(unsigned)blocks, threads, 0, st>>>(ctx, bt);
-   else k_group3<LA, LB, LC, LD, double><<<(unsigned)blocks, threads, 0, st>>>(ctx, bt);
+   if constexpr (class_has_fp32(LA, LB, LC, LD)) {
+      if (bt.fp32) {
+         k_group3<LA, LB, LC, LD, float><<<(unsigned)blocks, threads, 0, st>>>(ctx, bt);
+         return cudaGetLastError();
+      }
+   } else {
+      if (bt.fp32) return cudaErrorInvalidValue;   // no FP32 segments for these classes
+   }
+   k_group3<LA, LB, LC, LD, double><<<(unsigned)blocks, threads, 0, st>>>(ctx, bt);
    return cudaGetLastError();
 }
 
@@ -158,8 +165,10 @@ struct PartPreload {
          cudaFuncAttributes a;
          cudaError_t e = cudaFuncGetAttributes(&a, k_group3<(c >> 6) & 3, (c >> 4) & 3, (c >> 2) & 3, c & 3, double>);
          if (e != cudaSuccess) return e;
-         e = cudaFuncGetAttributes(&a, k_group3<(c >> 6) & 3, (c >> 4) & 3, (c >> 2) & 3, c & 3, float>);
-         if (e != cudaSuccess) return e;
+         if constexpr (class_has_fp32((c >> 6) & 3, (c >> 4) & 3, (c >> 2) & 3, c & 3)) {
+            e = cudaFuncGetAttributes(&a, k_group3<(c >> 6) & 3, (c >> 4) & 3, (c >> 2) & 3, c & 3, float>);
+            if (e != cudaSuccess) return e;
+         }
          return PartPreload<I + kGroup3Parts>::run();
       }
    }

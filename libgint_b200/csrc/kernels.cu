@@ -503,7 +503,15 @@ static __device__ __forceinline__ void sph_pass(const double *src, double *dst, 
 // q = t / n for t * n < 2^20, with M = 2^20 / n + 1 (all spherical indices here: t < 7^4, n <= 7^3)
 static __device__ __forceinline__ int div_small(int t, uint32_t M) { return (int)(((uint32_t)t * M) >> 20); }
 
-// One contraction row q (of group G) processed by NL cooperating lanes.
+// Synchronises the NL threads that share one row's workspace: a block (NL > 32), a warp, or none.
+template <int NL>
+static __device__ __forceinline__ void gsync() {
+   if constexpr (NL > 32) __syncthreads();
+   else if constexpr (NL > 1) __syncwarp();
+}
+
+// One contraction row q (of group G) processed by NL cooperating threads (a block, a warp or one
+// lane; `lane` is the thread's index among them).
 template <int NL, int ST>
 static __device__ __forceinline__ void group_body(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan *pl,
                                                   const GroupRec &G, uint32_t q, double *ws, double *cart, int lane,
@@ -516,7 +524,7 @@ static __device__ __forceinline__ void group_body(const DevCtx &ctx, const Batch
    {
       const int r = (int)(q - G.qrtt_off);
       const int ia = r / (nl1 * nl2 * nl3), ib = (r / (nl2 * nl3)) % nl1, ic = (r / nl3) % nl2, id = r % nl3;
-      for (int q = lane; q < Nc; q += NL) cart[q * ST] = 0.0;
+      for (int x = lane; x < Nc; x += NL) cart[x * ST] = 0.0;
       for (uint32_t s = 0; s < G.nshell; s++) {
          const ShellRec sh = bt.shells[G.shell_off + s];
          const BasisEnt ea = ctx.ents[sh.ent[0]], eb = ctx.ents[sh.ent[1]];
@@ -526,9 +534,9 @@ static __device__ __forceinline__ void group_body(const DevCtx &ctx, const Batch
          const double *Kc = ctx.pool + ec.k_off + ic * ec.np;
          const double *Kd = ctx.pool + ed.k_off + id * ed.np;
          // contraction over primitives (reference src/compute_ECO.cpp:131-212)
-         if constexpr (NL == 32) {
-            // the contraction coefficients of 32 primitives at a time, one per lane, then every
-            // lane sums its targets over them in primitive order
+         if constexpr (NL >= 32) {
+            // the contraction coefficients of 32 primitives at a time, one per thread, then every
+            // thread sums its targets over them in primitive order
             if (sh.nprm == 0)
                for (int j = lane; j < S; j += NL) ws[j] = 0.0;
             for (uint32_t p0 = 0; p0 < sh.nprm; p0 += 32) {
@@ -538,7 +546,7 @@ static __device__ __forceinline__ void group_body(const DevCtx &ctx, const Batch
                   kpw[lane] = __ldg(Ka + (code >> 24)) * __ldg(Kb + ((code >> 16) & 255)) *
                               __ldg(Kc + ((code >> 8) & 255)) * __ldg(Kd + (code & 255));
                }
-               __syncwarp();
+               gsync<NL>();
                const double *acp = bt.AC + (size_t)(sh.prm_off + p0) * S;
                for (int j = lane; j < S; j += NL) {
                   double a = p0 ? ws[j] : 0.0;
@@ -555,7 +563,7 @@ static __device__ __forceinline__ void group_body(const DevCtx &ctx, const Batch
                   for (; q < np; q++) { a += kpw[q] * __ldg(rp); rp += S; }
                   ws[j] = a;
                }
-               __syncwarp();
+               gsync<NL>();
             }
          } else {
             for (int j = lane; j < S; j += NL) {
@@ -569,7 +577,7 @@ static __device__ __forceinline__ void group_body(const DevCtx &ctx, const Batch
                ws[j * ST] = a;
             }
          }
-         if (NL > 1) __syncwarp();
+         gsync<NL>();
          double A[3], B[3], C[3], D[3], CDs[3];
          shell_geom(ctx, ea, eb, ec, ed, sh.n1, sh.n2, A, B, C, D, CDs);
          // HRR (reference src/compute_HRR.cpp:7-99), one precompiled instruction per element; the
@@ -596,10 +604,10 @@ static __device__ __forceinline__ void group_body(const DevCtx &ctx, const Batch
                   }
                }
             }
-            if (NL > 1) __syncwarp();
+            gsync<NL>();
          }
-         for (int q = lane; q < Nc; q += NL) cart[q * ST] += ws[(pl->out_off + q) * ST];
-         if (NL > 1) __syncwarp();
+         for (int x = lane; x < Nc; x += NL) cart[x * ST] += ws[(pl->out_off + x) * ST];
+         gsync<NL>();
       }
       // cartesian -> spherical, one centre at a time (a, b, c, d); the two halves of the
       // workspace take turns as the output, and l = 0 centres (a coefficient of 1) are skipped
@@ -617,7 +625,7 @@ static __device__ __forceinline__ void group_body(const DevCtx &ctx, const Batch
             if (ls[ctr] == 1) sph_pass<1, NL, ST>(sph, dst, npre, npost, lane);
             else if (ls[ctr] == 2) sph_pass<2, NL, ST>(sph, dst, npre, npost, lane);
             else sph_pass<3, NL, ST>(sph, dst, npre, npost, lane);
-            if (NL > 1) __syncwarp();
+            gsync<NL>();
             dims[ctr] = ns[ctr];
             sph = dst;
          }
@@ -653,7 +661,7 @@ static __device__ __forceinline__ void group_body(const DevCtx &ctx, const Batch
             atomicAdd(Km + Iac, iabcd * __ldg(Pm + Ibd));
          }
       }
-      if (NL > 1) __syncwarp();
+      gsync<NL>();
    }
 }
 
@@ -684,6 +692,30 @@ __global__ void __launch_bounds__(256, 3) k_group(DevCtx ctx, BatchArgs bt, int 
       if (bt.gflags && !__ldg(bt.gflags + gi)) continue;   // screened on an incremental replay
       const GroupRec G = bt.groups[gi];
       group_body<32, 1>(ctx, bt, pl, G, q, wbase, wbase + Hws, lane, hrec, kpw);
+   }
+}
+
+// one block of four warps per contraction row, all of them on one workspace (in shared memory, or
+// for the largest classes a slice of the global scratch per block): for the classes whose rows are
+// long chains of HRR levels with hundreds to thousands of elements each and which have few rows,
+// a warp per row leaves the GPU mostly idle and takes a level in many rounds
+__global__ void __launch_bounds__(kGroupBlockThreads) k_group_block(DevCtx ctx, BatchArgs bt, int ws_doubles,
+                                                                    int use_global) {
+   extern __shared__ __align__(16) double smem[];
+   const ClassPlan *pl = reinterpret_cast<const ClassPlan *>(smem);
+   load_plan(bt.plan, smem);
+   __syncthreads();
+   const int plan_doubles = (int)((sizeof(ClassPlan) + 15) / 16) * 2;
+   double *kpw = smem + plan_doubles;
+   double *ws = use_global ? bt.gscratch + (size_t)blockIdx.x * ws_doubles : kpw + kGroupKpDoubles;
+   const int Hws = max(pl->H, 2 * pl->Nc);
+   const uint2 *hrec = ctx.gprog + ctx.gprog[bt.cls].x;
+   const int lane = threadIdx.x & 31;
+   for (uint32_t q = blockIdx.x; q < bt.nqrtt; q += gridDim.x) {
+      const uint32_t gi = row_group_one(bt, q, lane);   // the same in every warp of the block
+      if (bt.gflags && !__ldg(bt.gflags + gi)) continue;   // screened on an incremental replay
+      const GroupRec G = bt.groups[gi];
+      group_body<kGroupBlockThreads, 1>(ctx, bt, pl, G, q, ws, ws + Hws, (int)threadIdx.x, hrec, kpw);
    }
 }
 
@@ -917,8 +949,10 @@ size_t group_global_scratch(const ClassPlan &hp, int *grid, int *warps) {
 }
 
 
-// Group-kernel choice: k_group3 (generated HRR, one lane per group) for the classes it covers,
-// then k_group_lane / k_group.
+// Group-kernel choice: k_group3 (generated HRR, one lane per row) for the classes it covers; for
+// the others on variant 0 k_group_block (one block per row) where the workspace is large and fits
+// a block's shared memory, k_group_lane for small workspaces, else k_group (one warp per row),
+// which variant 1 always takes.
 cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan &hp, cudaStream_t st) {
    if (bt.nqrtt == 0) return cudaSuccess;
    if (bt.group_variant == 0 || bt.fp32) {
@@ -927,6 +961,22 @@ cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan
    }
    if (bt.fp32) return cudaErrorInvalidValue;   // FP32 segments exist only for classes with k_group3
    const size_t wd = group_warp_doubles(hp);
+   if (bt.group_variant == 0 && wd >= (size_t)kGroupBlockMinDoubles) {
+      const size_t smem = group_hdr_bytes() + (kGroupKpDoubles + wd) * 8;
+      if (smem <= (size_t)std::min(max_dyn_smem(), 200 * 1024)) {
+         const long blocks = std::max(1L, std::min((long)bt.nqrtt, 148L * 16));
+         k_group_block<<<(unsigned)blocks, kGroupBlockThreads, smem, st>>>(ctx, bt, (int)wd, 0);
+         return cudaGetLastError();
+      }
+      if (bt.gscratch) {   // workspace in the global scratch, which holds group_global_scratch's count
+         int grid = 0, warps = 0;
+         group_global_scratch(hp, &grid, &warps);
+         const long blocks = std::max(1L, std::min((long)bt.nqrtt, (long)grid * warps));
+         k_group_block<<<(unsigned)blocks, kGroupBlockThreads, group_hdr_bytes() + kGroupKpDoubles * 8, st>>>(
+            ctx, bt, (int)wd, 1);
+         return cudaGetLastError();
+      }
+   }
    if (wd <= 40 && bt.group_variant == 0) {
       // small workspace: one lane per group, 32 groups per warp
       const int lane_doubles = (int)wd;
@@ -1120,7 +1170,7 @@ cudaError_t preload_kernels() {
    const int smax = max_dyn_smem();
    const void *fns[] = {(const void *)k_prim<1>, (const void *)k_prim<4>, (const void *)k_prim<8>,
                         (const void *)k_prim<32>, (const void *)k_prim2<true>, (const void *)k_prim2<false>,
-                        (const void *)k_group, (const void *)k_group_lane};
+                        (const void *)k_group, (const void *)k_group_lane, (const void *)k_group_block};
    for (const void *f : fns)
       if ((e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smax)) != cudaSuccess) return e;
    cudaFuncAttributes a;

@@ -72,6 +72,10 @@ cudaError_t launch_prim(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan 
 cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan &hp, cudaStream_t st);
 size_t group_global_scratch(const ClassPlan &hp, int *grid, int *warps);
 constexpr int kGroupKpDoubles = 32;   // per-warp shared buffer of contraction coefficients in k_group
+constexpr int kGroupBlockThreads = 128;   // k_group_block: threads sharing one row's workspace
+// k_group_block (variant 0) for the classes whose workspace holds at least this many doubles: on
+// the 64-molecule l <= 3 workload it was faster than one warp per row from about here on
+constexpr int kGroupBlockMinDoubles = 1536;
 int prim_team_size(const ClassPlan &hp);
 // Incremental replay screening (k_group_screen): mode 0 writes each group's largest |P| over the P
 // blocks its rows read into pmax (the recording's P); mode 1 sets flags[g] = 0 for the groups whose

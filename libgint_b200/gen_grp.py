@@ -31,7 +31,8 @@ from libgint_b200.gen_vrr import cart, cidx, first_dir, lowered, ncart, plan
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "csrc", "grp_gen.cuh")
 HMAX = 140
-LGMAX = 3      # one lane per group wins up to L = 3; larger classes keep the warp kernel
+LGMAX = 3      # one lane per contraction row up to L = 3; at L = 4 (up to 100 targets per lane,
+               # 255 registers with spills) it was slower than the warp kernels for most classes
 LMAX = 3
 
 # unnormalised real solid harmonics as integer coefficients on the cartesian monomials, rows
