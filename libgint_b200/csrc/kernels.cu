@@ -873,9 +873,11 @@ int prim_team_size(const ClassPlan &hp) {
    return 32;
 }
 
-// k_prim2 launch shape: primitives per warp chunk and the per-warp shared-memory size
+// k_prim2 launch shape: primitives per warp chunk and the per-warp shared-memory size. The chunk's
+// image-summed targets (cp x S doubles) are the largest part of a warp's shared memory, and
+// shared memory bounds the warps per SM of the large classes, so a chunk holds about 512 targets.
 static void prim2_shape(const ClassPlan &hp, bool lane_vrr, int *cp, size_t *warp_doubles) {
-   int c = std::max(1, std::min(32, 2048 / std::max(1, hp.S)));
+   int c = std::max(1, std::min(32, 512 / std::max(1, hp.S)));
    const size_t geo = (sizeof(PrimGeo) / 8);
    size_t w = geo * c + c + (size_t)c * hp.S + 32 + 64 + 32 + 64 * (size_t)(hp.L + 1) +
               (lane_vrr ? 17 * 32 + 32 * (size_t)hp.V : 18 + (size_t)hp.V + 2);
