@@ -672,8 +672,9 @@ static __device__ __forceinline__ void load_plan(const ClassPlan *src_plan, doub
    for (int w = threadIdx.x; w < nwords; w += blockDim.x) dst[w] = src[w];
 }
 
-// one warp per contraction row
-__global__ void __launch_bounds__(256, 3) k_group(DevCtx ctx, BatchArgs bt, int warp_doubles, int use_global) {
+// one warp per contraction row; the kernel waits on chains of dependent loads, so 64 registers
+// (32 warps per SM, a few spills) beat 80 (24 warps)
+__global__ void __launch_bounds__(256, 4) k_group(DevCtx ctx, BatchArgs bt, int warp_doubles, int use_global) {
    extern __shared__ __align__(16) double smem[];
    const ClassPlan *pl = reinterpret_cast<const ClassPlan *>(smem);
    load_plan(bt.plan, smem);
@@ -698,8 +699,9 @@ __global__ void __launch_bounds__(256, 3) k_group(DevCtx ctx, BatchArgs bt, int 
 // one block of four warps per contraction row, all of them on one workspace (in shared memory, or
 // for the largest classes a slice of the global scratch per block): for the classes whose rows are
 // long chains of HRR levels with hundreds to thousands of elements each and which have few rows,
-// a warp per row leaves the GPU mostly idle and takes a level in many rounds
-__global__ void __launch_bounds__(kGroupBlockThreads) k_group_block(DevCtx ctx, BatchArgs bt, int ws_doubles,
+// a warp per row leaves the GPU mostly idle and takes a level in many rounds. 64 registers: eight
+// blocks per SM
+__global__ void __launch_bounds__(kGroupBlockThreads, 8) k_group_block(DevCtx ctx, BatchArgs bt, int ws_doubles,
                                                                     int use_global) {
    extern __shared__ __align__(16) double smem[];
    const ClassPlan *pl = reinterpret_cast<const ClassPlan *>(smem);
