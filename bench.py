@@ -72,7 +72,7 @@ def parse():
                     help="OpenMP team size of the end-to-end leg (one handle per thread)")
     ap.add_argument("--device-only", action="store_true",
                     help="record and replay only (no end-to-end, CPU or reference legs)")
-    ap.add_argument("--max-mem-mb", type=int, default=40000,
+    ap.add_argument("--max-mem-mb", type=int, default=120000,
                     help="libgint_set_max_mem of the recording handle (large: few batches, one launch per class each)")
     ap.add_argument("--clusters-stride", type=int, default=64,
                     help="set-quartet sample of the batched-systems leg (0 = skip the leg)")
