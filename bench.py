@@ -80,8 +80,9 @@ def parse():
                     help="set-quartet sample of the SCF-loop leg (0 = skip the leg)")
     ap.add_argument("--fp32-threshold", type=float, default=1e-5,
                     help="Schwarz bound below which shell quartets run in FP32 (the mixed path)")
-    ap.add_argument("--host-mem-mb", type=int, default=300,
-                    help="libgint_set_max_mem of each end-to-end handle (smaller batches start the GPU sooner)")
+    ap.add_argument("--host-mem-mb", type=int, default=4000,
+                    help="libgint_set_max_mem of each end-to-end handle (large: few flushes and launches per "
+                         "thread; 16 handles hold about 58 GB of device memory)")
     ap.add_argument("--no-reference-cuda", action="store_true",
                     help="skip timing the reference CUDA library on a small sample")
     return ap.parse_args()
@@ -611,7 +612,7 @@ def run_ours(args, world, rank, local):
             "ms_per_scf_iter": e2e_ms_step,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms_step,
-                    "host_threads": args.host_threads,
+                    "host_threads": args.host_threads, "handle_max_mem_mb": args.host_mem_mb,
                     "caller": "OpenMP team, one handle per thread, shared K, mixed precision",
                     "max_dK_vs_device_mixed_build": e2e_dev},
             "gpu_launches": mixed["launches"],
