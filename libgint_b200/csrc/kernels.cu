@@ -510,12 +510,36 @@ static __device__ __forceinline__ void gsync() {
    else if constexpr (NL > 1) __syncwarp();
 }
 
-// One contraction row q (of group G) processed by NL cooperating threads (a block, a warp or one
-// lane; `lane` is the thread's index among them).
+// What the rows of one set quartet share for one shell quartet: its primitive range, the
+// coefficient rows of its four basis entries and the HRR displacements AB = A - B, CD = C - D.
+struct ShellShared {
+   uint32_t key;              // group index it was derived for (shell 0 of that group); ~0u: empty
+   uint32_t prm_off, nprm;
+   int k_off[4], np[4];
+   double AB[3], CD[3];
+};
+static_assert(sizeof(ShellShared) <= kGroupShellCacheDoubles * 8, "shell cache slot too small");
+
+static __device__ __forceinline__ void shell_shared(const DevCtx &ctx, const ShellRec &sh, ShellShared &o) {
+   const BasisEnt ea = ctx.ents[sh.ent[0]], eb = ctx.ents[sh.ent[1]];
+   const BasisEnt ec = ctx.ents[sh.ent[2]], ed = ctx.ents[sh.ent[3]];
+   o.prm_off = sh.prm_off; o.nprm = sh.nprm;
+   o.k_off[0] = ea.k_off; o.k_off[1] = eb.k_off; o.k_off[2] = ec.k_off; o.k_off[3] = ed.k_off;
+   o.np[0] = ea.np; o.np[1] = eb.np; o.np[2] = ec.np; o.np[3] = ed.np;
+   double A[3], B[3], C[3], D[3], CDs[3];
+   shell_geom(ctx, ea, eb, ec, ed, sh.n1, sh.n2, A, B, C, D, CDs);
+   for (int c = 0; c < 3; c++) { o.AB[c] = A[c] - B[c]; o.CD[c] = C[c] - D[c]; }
+}
+
+// One contraction row q (of group gi = G) processed by NL cooperating threads (a block, a warp or
+// one lane; `lane` is the thread's index among them). With a cache slot (one warp's shared memory,
+// key ~0u at first), shell 0's shared data is derived once and reused by the next rows of the
+// same group that this warp takes.
 template <int NL, int ST>
 static __device__ __forceinline__ void group_body(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan *pl,
                                                   const GroupRec &G, uint32_t q, double *ws, double *cart, int lane,
-                                                  const uint2 *hrec, double *kpw) {
+                                                  const uint2 *hrec, double *kpw, ShellShared *cache = nullptr,
+                                                  uint32_t gi = 0) {
    const int S = pl->S, Nc = pl->Nc, Ns = pl->Ns;
    const int la = pl->la, lb = pl->lb, lc = pl->lc, ld = pl->ld;
    const int nca = ncart(la), ncb = ncart(lb), ncc = ncart(lc), ncd_ = ncart(ld);
@@ -526,13 +550,21 @@ static __device__ __forceinline__ void group_body(const DevCtx &ctx, const Batch
       const int ia = r / (nl1 * nl2 * nl3), ib = (r / (nl2 * nl3)) % nl1, ic = (r / nl3) % nl2, id = r % nl3;
       for (int x = lane; x < Nc; x += NL) cart[x * ST] = 0.0;
       for (uint32_t s = 0; s < G.nshell; s++) {
-         const ShellRec sh = bt.shells[G.shell_off + s];
-         const BasisEnt ea = ctx.ents[sh.ent[0]], eb = ctx.ents[sh.ent[1]];
-         const BasisEnt ec = ctx.ents[sh.ent[2]], ed = ctx.ents[sh.ent[3]];
-         const double *Ka = ctx.pool + ea.k_off + ia * ea.np;
-         const double *Kb = ctx.pool + eb.k_off + ib * eb.np;
-         const double *Kc = ctx.pool + ec.k_off + ic * ec.np;
-         const double *Kd = ctx.pool + ed.k_off + id * ed.np;
+         ShellShared sh;
+         if (cache && s == 0 && cache->key == gi) {
+            sh = *cache;
+         } else {
+            shell_shared(ctx, bt.shells[G.shell_off + s], sh);
+            if (cache && s == 0) {
+               gsync<NL>();
+               if (lane == 0) { *cache = sh; cache->key = gi; }
+               gsync<NL>();
+            }
+         }
+         const double *Ka = ctx.pool + sh.k_off[0] + ia * sh.np[0];
+         const double *Kb = ctx.pool + sh.k_off[1] + ib * sh.np[1];
+         const double *Kc = ctx.pool + sh.k_off[2] + ic * sh.np[2];
+         const double *Kd = ctx.pool + sh.k_off[3] + id * sh.np[3];
          // contraction over primitives (reference src/compute_ECO.cpp:131-212)
          if constexpr (NL >= 32) {
             // the contraction coefficients of 32 primitives at a time, one per thread, then every
@@ -578,16 +610,14 @@ static __device__ __forceinline__ void group_body(const DevCtx &ctx, const Batch
             }
          }
          gsync<NL>();
-         double A[3], B[3], C[3], D[3], CDs[3];
-         shell_geom(ctx, ea, eb, ec, ed, sh.n1, sh.n2, A, B, C, D, CDs);
          // HRR (reference src/compute_HRR.cpp:7-99), one precompiled instruction per element; the
          // elements of one level are independent, so each lane loads four before it stores any
          for (int lv = 1; lv <= pl->nhlev; lv++) {
             const HOp h0 = pl->hop[pl->hlev_off[lv - 1]], h1 = pl->hop[pl->hlev_off[lv] - 1];
             const int x0 = h0.out, x1 = h1.out + h1.nelem;
             double R0, R1, R2;
-            if (h0.type == 0) { R0 = C[0] - D[0]; R1 = C[1] - D[1]; R2 = C[2] - D[2]; }
-            else { R0 = A[0] - B[0]; R1 = A[1] - B[1]; R2 = A[2] - B[2]; }
+            if (h0.type == 0) { R0 = sh.CD[0]; R1 = sh.CD[1]; R2 = sh.CD[2]; }
+            else { R0 = sh.AB[0]; R1 = sh.AB[1]; R2 = sh.AB[2]; }
             for (int x = x0 + lane; x < x1; x += 4 * NL) {
                uint2 ins[4];
 #pragma unroll
@@ -688,11 +718,24 @@ __global__ void __launch_bounds__(256, 4) k_group(DevCtx ctx, BatchArgs bt, int 
                               : (smem + plan_doubles + nwarp * kGroupKpDoubles + (size_t)warp * warp_doubles);
    const int Hws = max(pl->H, 2 * pl->Nc);
    const uint2 *hrec = ctx.gprog + ctx.gprog[bt.cls].x;
-   for (uint32_t q = gwarp; q < bt.nqrtt; q += gridDim.x * nwarp) {
-      const uint32_t gi = row_group_one(bt, q, lane);
-      if (bt.gflags && !__ldg(bt.gflags + gi)) continue;   // screened on an incremental replay
-      const GroupRec G = bt.groups[gi];
-      group_body<32, 1>(ctx, bt, pl, G, q, wbase, wbase + Hws, lane, hrec, kpw);
+   ShellShared *cache = reinterpret_cast<ShellShared *>(kpw + 32);
+   if (lane == 0) cache->key = ~0u;
+   __syncwarp();
+   // kGroupRowsPerWarp consecutive rows at a time, so that the rows of one set quartet that follow
+   // each other on this warp reuse its group record and shell 0's shared data
+   uint32_t gi = 0, gend = 0;
+   GroupRec G = {};
+   for (uint32_t q0 = gwarp * kGroupRowsPerWarp; q0 < bt.nqrtt; q0 += gridDim.x * nwarp * kGroupRowsPerWarp) {
+      const uint32_t q1 = min(q0 + kGroupRowsPerWarp, bt.nqrtt);
+      for (uint32_t q = q0; q < q1; q++) {
+         if (q >= gend || q < G.qrtt_off) {
+            gi = row_group_one(bt, q, lane);
+            G = bt.groups[gi];
+            gend = G.qrtt_off + (uint32_t)G.nl[0] * G.nl[1] * G.nl[2] * G.nl[3];
+         }
+         if (bt.gflags && !__ldg(bt.gflags + gi)) continue;   // screened on an incremental replay
+         group_body<32, 1>(ctx, bt, pl, G, q, wbase, wbase + Hws, lane, hrec, kpw, cache, gi);
+      }
    }
 }
 
@@ -996,7 +1039,7 @@ cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan
    const int nw = group_smem_warps(wd);
    if (nw >= 1) {
       const size_t smem = plan_bytes + (size_t)nw * (wd + kGroupKpDoubles) * 8;
-      long blocks = ((long)bt.nqrtt + nw - 1) / nw;
+      long blocks = ((long)bt.nqrtt + (long)nw * kGroupRowsPerWarp - 1) / ((long)nw * kGroupRowsPerWarp);
       blocks = std::max(1L, std::min(blocks, 148L * 64));
       k_group<<<(unsigned)blocks, nw * 32, smem, st>>>(ctx, bt, (int)wd, 0);
    } else {

@@ -71,7 +71,11 @@ cudaError_t upload_constant_tables(const double *c2s_l0to3, const double *symm5)
 cudaError_t launch_prim(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan &hp, cudaStream_t st);
 cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan &hp, cudaStream_t st);
 size_t group_global_scratch(const ClassPlan &hp, int *grid, int *warps);
-constexpr int kGroupKpDoubles = 32;   // per-warp shared buffer of contraction coefficients in k_group
+// per-warp shared buffer of k_group: 32 contraction coefficients, then a slot that keeps shell 0's
+// shared data (records, basis entries, displacements) for the next rows of the same set quartet
+constexpr int kGroupShellCacheDoubles = 16;
+constexpr int kGroupKpDoubles = 32 + kGroupShellCacheDoubles;
+constexpr int kGroupRowsPerWarp = 4;      // consecutive rows a warp of k_group takes at a time
 constexpr int kGroupBlockThreads = 128;   // k_group_block: threads sharing one row's workspace
 // k_group_block (variant 0) for the classes whose workspace holds at least this many doubles: on
 // the 64-molecule l <= 3 workload it was faster than one warp per row from about here on
