@@ -68,8 +68,9 @@ def parse():
     ap.add_argument("--setq-stride", type=int, default=512,
                     help="process a uniform 1/stride sample of the set quartets (1 = all)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--host-threads", type=int, default=min(16, os.cpu_count() or 1),
-                    help="OpenMP team size of the end-to-end leg (one handle per thread)")
+    ap.add_argument("--host-threads", type=int, default=0,
+                    help="OpenMP team size of the end-to-end leg per rank (one handle per thread; "
+                         "0: the host's cores shared among the ranks, at most 16)")
     ap.add_argument("--device-only", action="store_true",
                     help="record and replay only (no end-to-end, CPU or reference legs)")
     ap.add_argument("--max-mem-mb", type=int, default=120000,
@@ -197,7 +198,7 @@ def run_reference(args, world, rank):
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": workload_desc(args, wl), "sample": sample},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -375,6 +376,8 @@ def run_ours(args, world, rank, local):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
         pg = True
 
+    if args.host_threads <= 0:
+        args.host_threads = max(1, min(16, (os.cpu_count() or 1) // world))
     lib = load_engine()
     t_gen = time.perf_counter()
     wl = make_workload(args)
@@ -590,7 +593,7 @@ def run_ours(args, world, rank, local):
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": mixed["ms"], "higher_is_better": True,
-            "scaling": "weak" if world > 1 else "strong", "vs_baseline": None, "dtype": "f32/f64",
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32/f64",
             "data": "synthetic",
             "config": {"workload": workload_desc(args, wl),
                        "shell_quartets": total_shells, "primitive_quartets": wl.info["n_prims"],
