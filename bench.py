@@ -424,7 +424,7 @@ def run_ours(args, world, rank, local):
         try:
             sess = Session(api, wl, max_mem_mb=args.max_mem_mb)
             h = ctypes.c_void_p(sess.h)
-            lib.libgint_record(h, 1)
+            lib.libgint_record(h, 2)
             K_rec, ms_rec, _ = sess.build_K_subset(idx)
             lib.libgint_record(h, 0)
         finally:
@@ -449,9 +449,13 @@ def run_ours(args, world, rank, local):
         K = np.zeros_like(K_rec)
         lib.libgint_get_K(h, K.ctypes.data_as(D))
         check(h)
-        # the replayed K (same P) must be the streamed build's, checked on the timed replays' result
+        # the replayed K (same P) must be the streamed build's, checked on the timed replays' result.
+        # Both sum the same terms in another order (atomics; the merged replay runs its classes in
+        # other launches): on this ill-conditioned basis (terms up to 1e7-1e8 max|K| in the oracle's
+        # magnitude mode) that moves K by up to ~1e-10 max|K|, while a lost or doubled class
+        # segment moves it by orders of magnitude more
         dev = max_over_ranks(float(np.abs(K - K_rec).max() / max(1e-300, np.abs(K_rec).max())))
-        if not dev <= 1e-12:
+        if not dev <= 1e-10:
             raise RuntimeError(f"replayed K differs from the streamed build's K: rel max|dK| = {dev:.3e}")
         lib.libgint_get_stats(h, stats)
         launches = (stats[4] - launches0) // max(1, args.steps)

@@ -138,10 +138,14 @@ int libgint_hrr_program(int la, int lb, int lc, int ld, unsigned int *out, int c
  * (0|0)^(m) count at w[0..], ntg, then per target {workspace offset, target offset, length, e, f},
  * info_cap >= 4 + 5 ntg. Returns the instruction count (-1: unsupported class). No GPU needed. */
 int libgint_vrr_program(int la, int lb, int lc, int ld, void *vops, int cap, int *info, int info_cap);
-/* on = 1: keep the device batches of the following K build(s) (the screened quartet list of
- * an SCF step); on = 0: stop recording. libgint_replay captures the whole replay (every class
- * segment's kernels on the worker streams) into a CUDA graph once and relaunches it while the
- * recording, P/K buffers and kernel choices stay the same. */
+/* No counterpart in the reference. on = 1: keep the device batches of the following K build(s)
+ * (the screened quartet list of an SCF step); on = 2: the same, and when the recording stops the
+ * batches' segments of each class are merged into one (a replay then launches two kernels per
+ * class instead of two per class and batch; skipped if the merged batch would need more replay
+ * memory than two batch-sized halves, and it briefly holds the recording twice); on = 0: stop
+ * recording. libgint_replay captures the whole replay (every class segment's kernels on the worker
+ * streams) into a CUDA graph once and relaunches it while the recording, P/K buffers and kernel
+ * choices stay the same. */
 void libgint_record(void *handle, int on);
 /* recompute K from the recorded quartet list with the current P (after libgint_set_P), without
  * the add_* stream; K is then read with libgint_get_K. Returns the device time in ms. */

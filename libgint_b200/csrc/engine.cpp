@@ -312,6 +312,7 @@ struct Handle {
    // largest |P| of the recording (float) and incremental-replay flags (byte) at g_pmax[i], g_flag[i]
    struct RecBatch { DBuf rec, gbuf; std::vector<RecSeg> segs; std::vector<size_t> g_pmax, g_flag; size_t ac_doubles = 0; };
    bool recording = false;
+   bool merge_rec = false;          // libgint_record(h, 2): one segment per queue class at the end
    std::vector<RecBatch> recs;
    long long rec_gen = 0;           // bumped whenever the recording changes
    // the replay captured as a CUDA graph, and what it was captured with
@@ -980,6 +981,83 @@ static double replay_impl(Handle *h, double *kt, double *kcls = nullptr, double 
 
 // After a recording: per recorded segment, each group's largest |P| over the blocks its rows read,
 // with the recording's P (for the screening of incremental replays, libgint_replay_incremental).
+// libgint_record(h, 2) at the end of the recording: the segments of each queue class in all the
+// recorded batches become one segment of one batch, so that a replay launches two kernels per class
+// instead of two per class and batch. The parts are copied device to device in batch order (so
+// every row, shell and primitive keeps its relative order) and their segment-relative indices are
+// shifted (launch_rebase_part); the per-32-row group table is rebuilt. Skipped (the batches stay as
+// recorded) when the merged batch would need more replay AC memory than the two alternating
+// batch-sized halves that a multi-batch replay holds.
+static bool merge_recording(Handle *h) {
+   if (h->err || h->recs.size() < 2) return !h->err;
+   size_t ac_max = 0;
+   for (auto &rb : h->recs) ac_max = std::max(ac_max, rb.ac_doubles);
+   std::vector<int> order;
+   std::vector<std::vector<std::pair<size_t, size_t>>> parts(2 * 256);
+   for (size_t bi = 0; bi < h->recs.size(); bi++)
+      for (size_t si = 0; si < h->recs[bi].segs.size(); si++) {
+         const int c = h->recs[bi].segs[si].c;
+         if (parts[c].empty()) order.push_back(c);
+         parts[c].push_back({bi, si});
+      }
+   Handle::RecBatch m;
+   size_t off = 0, ac = 0;
+   for (int c : order) {
+      Handle::RecSeg g;
+      std::memset(&g, 0, sizeof(g));
+      g.c = c;
+      for (auto &pr : parts[c]) {
+         const auto &s = h->recs[pr.first].segs[pr.second];
+         g.nprm += s.nprm; g.nshell += s.nshell; g.ngroup += s.ngroup; g.nqrtt += s.nqrtt;
+      }
+      g.o_prm = off; off = al16(off + (size_t)g.nprm * 4);
+      g.o_ps = off; off = al16(off + (size_t)g.nprm * 4);
+      g.o_sh = off; off = al16(off + (size_t)g.nshell * sizeof(ShellRec));
+      g.o_g = off; off = al16(off + (size_t)g.ngroup * sizeof(GroupRec));
+      g.o_q = off; off = al16(off + (size_t)g.nqrtt * sizeof(QrttRec));
+      g.o_rg = off; off = al16(off + ((size_t)g.nqrtt + 31) / 32 * 4);
+      g.ac_off = ac;
+      ac += ((size_t)g.nprm * h->plans[c & 255].S + 1) & ~(size_t)1;
+      m.segs.push_back(g);
+   }
+   if (ac > 2 * ac_max) return true;
+   if (!ensure(h, m.rec, std::max<size_t>(off, 256), "merged recording")) return false;
+   m.ac_doubles = ac;
+   char *dst = (char *)m.rec.p;
+   for (size_t k = 0; k < order.size(); k++) {
+      const Handle::RecSeg &g = m.segs[k];
+      uint32_t pb = 0, sb = 0, gb = 0, qb = 0;
+      for (auto &pr : parts[g.c]) {
+         const auto &s = h->recs[pr.first].segs[pr.second];
+         const char *src = (const char *)h->recs[pr.first].rec.p;
+         auto cp = [&](size_t to, size_t from, size_t bytes) {
+            return !bytes || ck(h, cudaMemcpyAsync(dst + to, src + from, bytes, cudaMemcpyDeviceToDevice, h->stream),
+                                "merged recording copy");
+         };
+         if (!cp(g.o_prm + (size_t)pb * 4, s.o_prm, (size_t)s.nprm * 4) ||
+             !cp(g.o_ps + (size_t)pb * 4, s.o_ps, (size_t)s.nprm * 4) ||
+             !cp(g.o_sh + (size_t)sb * sizeof(ShellRec), s.o_sh, (size_t)s.nshell * sizeof(ShellRec)) ||
+             !cp(g.o_g + (size_t)gb * sizeof(GroupRec), s.o_g, (size_t)s.ngroup * sizeof(GroupRec)) ||
+             !cp(g.o_q + (size_t)qb * sizeof(QrttRec), s.o_q, (size_t)s.nqrtt * sizeof(QrttRec)))
+            return false;
+         if ((pb || sb || gb || qb) &&
+             !ck(h, launch_rebase_part((uint32_t *)(dst + g.o_ps) + pb, s.nprm, (ShellRec *)(dst + g.o_sh) + sb,
+                                       s.nshell, (GroupRec *)(dst + g.o_g) + gb, s.ngroup, pb, sb, gb, qb, h->stream),
+                 "merged recording rebase"))
+            return false;
+         pb += s.nprm; sb += s.nshell; gb += s.ngroup; qb += s.nqrtt;
+      }
+      if (!ck(h, launch_row_groups((const GroupRec *)(dst + g.o_g), g.ngroup, (uint32_t *)(dst + g.o_rg), h->stream),
+              "merged recording row table"))
+         return false;
+   }
+   if (!ck(h, cudaStreamSynchronize(h->stream), "merged recording")) return false;
+   for (auto &rb : h->recs) { release(rb.rec); release(rb.gbuf); }
+   h->recs.clear();
+   h->recs.push_back(m);
+   return true;
+}
+
 static void record_group_pmax(Handle *h) {
    if (h->err || h->recs.empty() || !h->team || !h->team->ok) return;
    use_device(h);
@@ -1610,7 +1688,8 @@ void libgint_host_tables(double *ftable, double *c2s, unsigned char *lut, double
 }
 
 // Record the device batches of the following K build(s) so that libgint_replay can recompute
-// K for a new P without the add_* stream (on = 1 starts a new recording, 0 stops).
+// K for a new P without the add_* stream (on = 1 starts a new recording, 2 one whose batches are
+// merged into one segment per class when it stops, 0 stops).
 void libgint_record(void *hh, int on) {
    Handle *h = (Handle *)hh;
    if (on) {
@@ -1620,7 +1699,6 @@ void libgint_record(void *hh, int on) {
       h->recs.clear();
    } else {
       flush(h);
-      record_group_pmax(h);
       // the streaming slots' buffers are not needed to replay; release them, so that a recording's
       // replays hold the recorded batches and the replay buffers only (a streamed build allocates
       // them again)
@@ -1631,8 +1709,11 @@ void libgint_record(void *hh, int on) {
             release(sl.rec); release(sl.ac); release(sl.gscr);
          }
       }
+      if (h->merge_rec) merge_recording(h);
+      record_group_pmax(h);
    }
    h->recording = on != 0;
+   if (on) h->merge_rec = on == 2;
    h->rec_gen++;
 }
 

@@ -1131,6 +1131,48 @@ cudaError_t launch_tile_max(const double *P, size_t n, float *tmax, cudaStream_t
 
 size_t tile_max_count(size_t n) { return (n + kScreenTile - 1) / kScreenTile; }
 
+// ---------------------------------------------------------------------------------------
+// Merging the recorded batches of one queue class into one segment (libgint_record(h, 2)): the
+// parts are copied one after another, then the indices that count within a segment are shifted
+// by the part's position in the merged segment, and the per-32-row group table is rebuilt.
+// ---------------------------------------------------------------------------------------
+__global__ void k_rebase_part(uint32_t *prm_shell, uint32_t nprm, ShellRec *shells, uint32_t nshell, GroupRec *groups,
+                              uint32_t ngroup, uint32_t prm_base, uint32_t shell_base, uint32_t group_base,
+                              uint32_t qrtt_base) {
+   const uint32_t n = max(nprm, max(nshell, ngroup));
+   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+      if (i < nprm) prm_shell[i] += shell_base;
+      if (i < nshell) { shells[i].prm_off += prm_base; shells[i].group += group_base; }
+      if (i < ngroup) { groups[i].shell_off += shell_base; groups[i].qrtt_off += qrtt_base; }
+   }
+}
+
+__global__ void k_row_groups(const GroupRec *groups, uint32_t ngroup, uint32_t *rowgrp) {
+   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < ngroup; g += gridDim.x * blockDim.x) {
+      const GroupRec G = groups[g];
+      const uint32_t end = G.qrtt_off + (uint32_t)G.nl[0] * G.nl[1] * G.nl[2] * G.nl[3];
+      for (uint32_t k = (G.qrtt_off + 31) / 32; 32 * k < end; k++) rowgrp[k] = g;
+   }
+}
+
+cudaError_t launch_rebase_part(uint32_t *prm_shell, uint32_t nprm, ShellRec *shells, uint32_t nshell, GroupRec *groups,
+                               uint32_t ngroup, uint32_t prm_base, uint32_t shell_base, uint32_t group_base,
+                               uint32_t qrtt_base, cudaStream_t st) {
+   const uint32_t n = std::max(nprm, std::max(nshell, ngroup));
+   if (n == 0) return cudaSuccess;
+   const long blocks = std::max(1L, std::min((long)((n + 255) / 256), 148L * 16));
+   k_rebase_part<<<(unsigned)blocks, 256, 0, st>>>(prm_shell, nprm, shells, nshell, groups, ngroup, prm_base,
+                                                   shell_base, group_base, qrtt_base);
+   return cudaGetLastError();
+}
+
+cudaError_t launch_row_groups(const GroupRec *groups, uint32_t ngroup, uint32_t *rowgrp, cudaStream_t st) {
+   if (ngroup == 0) return cudaSuccess;
+   const long blocks = std::max(1L, std::min((long)((ngroup + 255) / 256), 148L * 16));
+   k_row_groups<<<(unsigned)blocks, 256, 0, st>>>(groups, ngroup, rowgrp);
+   return cudaGetLastError();
+}
+
 cudaError_t launch_group_screen(const DevCtx &ctx, const BatchArgs &bt, float *pmax, uint8_t *flags, double eps,
                                 int mode, const float *tmax, cudaStream_t st) {
    if (bt.ngroup == 0) return cudaSuccess;
@@ -1222,6 +1264,8 @@ cudaError_t preload_kernels() {
       if ((e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smax)) != cudaSuccess) return e;
    cudaFuncAttributes a;
    if ((e = cudaFuncGetAttributes(&a, (const void *)k_fp64_fma)) != cudaSuccess) return e;
+   if ((e = cudaFuncGetAttributes(&a, (const void *)k_rebase_part)) != cudaSuccess) return e;
+   if ((e = cudaFuncGetAttributes(&a, (const void *)k_row_groups)) != cudaSuccess) return e;
    if ((e = prim3_preload(smax)) != cudaSuccess) return e;
    if ((e = group3_preload()) != cudaSuccess) return e;
    return group_prog_load();

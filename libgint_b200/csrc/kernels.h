@@ -90,6 +90,13 @@ cudaError_t launch_group_screen(const DevCtx &ctx, const BatchArgs &bt, float *p
 // maxima of |P| over consecutive tiles of 32 elements (an upper bound, rounded up), tile_max_count(n)
 cudaError_t launch_tile_max(const double *P, size_t n, float *tmax, cudaStream_t st);
 size_t tile_max_count(size_t n);
+// merging a queue class's recorded batches into one segment: shift the segment-relative indices
+// of a part copied at (prm_base, shell_base, group_base, qrtt_base), and rebuild the group of
+// every 32nd row of a merged segment
+cudaError_t launch_rebase_part(uint32_t *prm_shell, uint32_t nprm, ShellRec *shells, uint32_t nshell, GroupRec *groups,
+                               uint32_t ngroup, uint32_t prm_base, uint32_t shell_base, uint32_t group_base,
+                               uint32_t qrtt_base, cudaStream_t st);
+cudaError_t launch_row_groups(const GroupRec *groups, uint32_t ngroup, uint32_t *rowgrp, cudaStream_t st);
 // whether k_prim3 (generated VRR) covers class cls (prim3.cu)
 bool prim_has_generated(int cls);
 // classes with an FP32 path (generated VRR and HRR code): la + lb + lc + ld <= 3

@@ -4,7 +4,7 @@
                                        [--fp32-threshold 0] [--replays 3] [--autotune]
 
 streams the sampled set quartets of a named workload through the engine once with recording on
-(``libgint_record``), then replays the recording ``--replays`` times as a CUDA graph and once more
+(``libgint_record``, batches merged per class), then replays the recording ``--replays`` times as a CUDA graph and once more
 with the kernels serialised (``libgint_replay_profile``), and prints one JSON line: replay times,
 the prim/group family times of the serialised replay, shell quartets and launches per replay.
 A profiler skips the streamed build's and the warm-up replay's launches with ``-s`` (their counts
@@ -37,7 +37,7 @@ def main(argv=None):
     try:
         sess = Session(Api(engine_path()), wl, max_mem_mb=args.max_mem_mb)
         h = ctypes.c_void_p(sess.h)
-        lib.libgint_record(h, 1)
+        lib.libgint_record(h, 2)
         K0, _, _ = sess.build_K()
         lib.libgint_record(h, 0)
     finally:
@@ -66,7 +66,9 @@ def main(argv=None):
                       "launches_per_replay": per_replay, "launches_before_timed": before_timed,
                       "replay_vs_stream_rel_dK": dev, "error": int(err)}), flush=True)
     sess.close()
-    if err or not dev <= 1e-12:
+    # the same terms summed in another order: on the ill-conditioned l <= 3 basis that moves K by up
+    # to ~1e-10 max|K|; a lost or doubled class segment moves it by far more
+    if err or not dev <= 1e-10:
         raise SystemExit(1)
 
 
