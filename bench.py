@@ -228,7 +228,7 @@ def group_flops(lib, wl):
 def scf_leg(args, lib, api):
     """The SCF-loop workload (128 molecules, 15.6 A cell, the 256 nearest image cells, l <= 3 basis),
     on a uniform 1/--scf-stride sample of its set quartets: the quartet list is recorded once with
-    P_0 (mixed precision, --max-mem-mb 7000 recording budget), then 10 K updates follow
+    P_0 (mixed precision, 7000 MB recording budget, batches merged per class), then 10 K updates follow
     P_k = P_0 + eps_k sym(N(0,1)), eps_k log-spaced from 1e-2 to 1e-6, each one
     K_k = K_{k-1} + K(P_k - P_{k-1}) from the recording with incremental dP screening at the Schwarz
     threshold 1e-11 (libgint_replay_incremental, one CUDA graph). Device time per iteration; the
@@ -244,7 +244,7 @@ def scf_leg(args, lib, api):
     try:
         s = Session(api, wl, max_mem_mb=7000)
         h = ctypes.c_void_p(s.h)
-        lib.libgint_record(h, 1)
+        lib.libgint_record(h, 2)
         K, _, _ = s.build_K()
         lib.libgint_record(h, 0)
     finally:

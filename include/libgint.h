@@ -141,8 +141,7 @@ int libgint_vrr_program(int la, int lb, int lc, int ld, void *vops, int cap, int
 /* No counterpart in the reference. on = 1: keep the device batches of the following K build(s)
  * (the screened quartet list of an SCF step); on = 2: the same, and when the recording stops the
  * batches' segments of each class are merged into one (a replay then launches two kernels per
- * class instead of two per class and batch; skipped if the merged batch would need more replay
- * memory than two batch-sized halves, and it briefly holds the recording twice); on = 0: stop
+ * class instead of two per class and batch; while it merges it holds the recording twice); on = 0: stop
  * recording. libgint_replay captures the whole replay (every class segment's kernels on the worker
  * streams) into a CUDA graph once and relaunches it while the recording, P/K buffers and kernel
  * choices stay the same. */

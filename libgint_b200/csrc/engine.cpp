@@ -254,7 +254,6 @@ struct Handle {
    cudaStream_t work[kWorkStreams] = {};
    cudaEvent_t work_ev[kWorkStreams] = {};
    cudaEvent_t fork_ev = nullptr;
-   cudaEvent_t batch_ev[2][kWorkStreams] = {};   // replay: each worker's end of the last batch of each parity
    cudaEvent_t noalloc_ev = nullptr;             // libgint_replay_noalloc: the caller's stream waits for the handle's
    int err = 0;
    std::string errmsg;
@@ -307,10 +306,10 @@ struct Handle {
    Slot slots[2];
    int cur = 0;
    // record / replay of the device-resident quartet list
-   struct RecSeg { int c; size_t o_prm, o_ps, o_sh, o_g, o_q, o_rg, ac_off; uint32_t nprm, nshell, ngroup, nqrtt; };
+   struct RecSeg { int c; size_t o_prm, o_ps, o_sh, o_g, o_q, o_rg; uint32_t nprm, nshell, ngroup, nqrtt; };
    // per recorded batch: its records, its class segments, and (gbuf) each segment's per-group
    // largest |P| of the recording (float) and incremental-replay flags (byte) at g_pmax[i], g_flag[i]
-   struct RecBatch { DBuf rec, gbuf; std::vector<RecSeg> segs; std::vector<size_t> g_pmax, g_flag; size_t ac_doubles = 0; };
+   struct RecBatch { DBuf rec, gbuf; std::vector<RecSeg> segs; std::vector<size_t> g_pmax, g_flag; };
    bool recording = false;
    bool merge_rec = false;          // libgint_record(h, 2): one segment per queue class at the end
    std::vector<RecBatch> recs;
@@ -321,6 +320,7 @@ struct Handle {
    GraphKey graph_key;
    long long graph_launches = 0;
    DBuf rec_ac, rec_gscr;
+   size_t arena_off[kWorkStreams] = {};   // replay: each worker stream's AC arena in rec_ac (doubles)
    // optional device event counters [256 classes][4]
    DBuf d_cnt;
    bool counting = false;
@@ -530,6 +530,16 @@ static cudaStream_t worker_for(Handle *h, int i, bool uses_scratch) {
    return uses_scratch ? h->work[0] : h->work[1 + i % (kWorkStreams - 1)];
 }
 
+// The worker stream (index) that a replay gives its i-th recorded segment (of class c), as
+// worker_for does, and the image-summed targets that segment needs (doubles, 32-byte multiple).
+static int replay_worker(Handle *h, int c, int i) {
+   int a, b;
+   return group_global_scratch(h->plans[c & 255], &a, &b) != 0 ? 0 : 1 + i % (kWorkStreams - 1);
+}
+static size_t replay_seg_ac(Handle *h, int c, uint32_t nprm) {
+   return ((size_t)nprm * h->plans[c & 255].S + 3) & ~(size_t)3;
+}
+
 static DevCtx make_ctx(Handle *h) {
    DevCtx c;
    std::memset(&c, 0, sizeof(c));
@@ -633,7 +643,6 @@ static void flush(Handle *h) {
       rb = &h->recs.back();
       if (!ensure(h, rb->rec, off, "recorded batch")) return;
       dev_rec = (char *)rb->rec.p;
-      rb->ac_doubles = ac;
    }
    for (const Seg &g : segs) {
       ClassQ &Q = h->q[g.c];
@@ -685,7 +694,7 @@ static void flush(Handle *h) {
       if (!ck(h, launch_prim(ctx, bt, hp, ws), "k_prim launch")) return;
       if (!ck(h, launch_group(ctx, bt, hp, ws), "k_group launch")) return;
       h->n_launch += 2;
-      if (rb) rb->segs.push_back({g.c, g.o_prm, g.o_ps, g.o_sh, g.o_g, g.o_q, g.o_rg, g.ac_off, bt.nprm, bt.nshell, bt.ngroup, bt.nqrtt});
+      if (rb) rb->segs.push_back({g.c, g.o_prm, g.o_ps, g.o_sh, g.o_g, g.o_q, g.o_rg, bt.nprm, bt.nshell, bt.ngroup, bt.nqrtt});
       h->n_prims += bt.nprm; h->n_shells += bt.nshell; h->n_groups += bt.ngroup;
       if (bt.fp32) { h->n_prims_fp32 += bt.nprm; h->n_shells_fp32 += bt.nshell; }
    }
@@ -830,11 +839,6 @@ static bool enqueue_replay(Handle *h, const DevCtx &ctx, size_t ac, std::vector<
    for (size_t bi = 0; bi < h->recs.size(); bi++) {
       auto &rb = h->recs[bi];
       char *base = (char *)rb.rec.p;
-      double *ac_half = (double *)h->rec_ac.p + (bi & 1) * ac;
-      if (spread && bi >= 2)
-         for (int w = 0; w < kWorkStreams; w++)
-            for (int w2 = 0; w2 < kWorkStreams; w2++)
-               if (!ck(h, cudaStreamWaitEvent(h->work[w], h->batch_ev[bi & 1][w2], 0), "stream wait")) return false;
       for (size_t si = 0; si < rb.segs.size(); si++) {
          const auto &g = rb.segs[si];
          BatchArgs bt;
@@ -851,11 +855,13 @@ static bool enqueue_replay(Handle *h, const DevCtx &ctx, size_t ac, std::vector<
          bt.qrtts = (const QrttRec *)(base + g.o_q);
          bt.rowgrp = (const uint32_t *)(base + g.o_rg);
          bt.nprm = g.nprm; bt.nshell = g.nshell; bt.ngroup = g.ngroup; bt.nqrtt = g.nqrtt;
-         bt.AC = ac_half + g.ac_off;
+         // the segment's targets live in its worker stream's arena: the segments of one stream run
+         // one after another, and no other stream touches that arena
+         const int w = replay_worker(h, g.c, nseg++);
+         bt.AC = (double *)h->rec_ac.p + h->arena_off[w];
          bt.gscratch = (double *)h->rec_gscr.p;
-         int a_, b_;
          const ClassPlan &hp = h->plans[g.c & 255];
-         cudaStream_t st = spread ? worker_for(h, nseg++, group_global_scratch(hp, &a_, &b_) != 0) : h->stream;
+         cudaStream_t st = spread ? h->work[w] : h->stream;
          if (eps >= 0.0) {
             char *gb = (char *)rb.gbuf.p;
             uint8_t *flags = (uint8_t *)(gb + rb.g_flag[si]);
@@ -873,9 +879,6 @@ static bool enqueue_replay(Handle *h, const DevCtx &ctx, size_t ac, std::vector<
          kmark();
          *nlaunch += 2;
       }
-      if (spread)
-         for (int w = 0; w < kWorkStreams; w++)
-            if (!ck(h, cudaEventRecord(h->batch_ev[bi & 1][w], h->work[w]), "event record")) return false;
    }
    if (spread) join_workers(h);
    return !h->err;
@@ -891,26 +894,28 @@ static void drop_graph(Handle *h) {
 // once into a CUDA graph (the whole K build: every class segment's two kernels on the worker
 // streams, with their batch-to-batch dependencies) and relaunched as one graph while the recording
 // and the device pointers it was captured with stay the same.
-// Checks that a replay can run and sizes its buffers; *half = the AC buffer's half size.
+// Checks that a replay can run and sizes its buffers; *half = the replay AC buffer's size (doubles).
 static bool prepare_replay(Handle *h, size_t *half) {
    if (h->err) return false;
    use_device(h);
    if (h->recs.empty()) { set_error(h, 4, "libgint_replay: nothing recorded"); return false; }
    if (!h->team || !h->team->ok) { set_error(h, 4, "libgint_replay: call libgint_set_P first"); return false; }
    if (!upload_tables(h)) return false;
-   size_t ac = 0, gs = 0;
-   for (auto &rb : h->recs) {
-      ac = std::max(ac, rb.ac_doubles);
-      for (auto &g : rb.segs) { int a, b; gs = std::max(gs, group_global_scratch(h->plans[g.c & 255], &a, &b)); }
-   }
-   // Every batch numbers its AC rows from 0, and the worker streams run the segments of
-   // consecutive batches at the same time, so batches alternate between two halves of the replay
-   // AC buffer (as the streamed build alternates two slots), and batch b + 2, which reuses batch b's
-   // half, starts on each worker only after every worker has finished batch b. A recording of one
-   // batch needs one half.
-   ac = (ac + 3) & ~(size_t)3;
-   const size_t halves = h->recs.size() > 1 ? 2 : 1;
-   if (!ensure(h, h->rec_ac, std::max<size_t>(halves * ac * 8, 256), "replay AC")) return false;
+   // The replay runs the recorded segments in order on the worker streams (replay_worker); the
+   // segments of one stream run one after another, so each stream needs one AC arena as large as
+   // the largest segment it runs, and the streams' arenas are disjoint.
+   size_t arena[kWorkStreams] = {}, gs = 0;
+   int i = 0;
+   for (auto &rb : h->recs)
+      for (auto &g : rb.segs) {
+         const int w = replay_worker(h, g.c, i++);
+         arena[w] = std::max(arena[w], replay_seg_ac(h, g.c, g.nprm));
+         int a, b;
+         gs = std::max(gs, group_global_scratch(h->plans[g.c & 255], &a, &b));
+      }
+   size_t ac = 0;
+   for (int w = 0; w < kWorkStreams; w++) { h->arena_off[w] = ac; ac += arena[w]; }
+   if (!ensure(h, h->rec_ac, std::max<size_t>(ac * 8, 256), "replay AC")) return false;
    if (gs && !ensure(h, h->rec_gscr, gs * 8, "replay HRR scratch")) return false;
    *half = ac;
    return true;
@@ -985,13 +990,10 @@ static double replay_impl(Handle *h, double *kt, double *kcls = nullptr, double 
 // recorded batches become one segment of one batch, so that a replay launches two kernels per class
 // instead of two per class and batch. The parts are copied device to device in batch order (so
 // every row, shell and primitive keeps its relative order) and their segment-relative indices are
-// shifted (launch_rebase_part); the per-32-row group table is rebuilt. Skipped (the batches stay as
-// recorded) when the merged batch would need more replay AC memory than the two alternating
-// batch-sized halves that a multi-batch replay holds.
+// shifted (launch_rebase_part); the per-32-row group table is rebuilt. While it copies, the
+// recording is held twice.
 static bool merge_recording(Handle *h) {
    if (h->err || h->recs.size() < 2) return !h->err;
-   size_t ac_max = 0;
-   for (auto &rb : h->recs) ac_max = std::max(ac_max, rb.ac_doubles);
    std::vector<int> order;
    std::vector<std::vector<std::pair<size_t, size_t>>> parts(2 * 256);
    for (size_t bi = 0; bi < h->recs.size(); bi++)
@@ -1001,7 +1003,7 @@ static bool merge_recording(Handle *h) {
          parts[c].push_back({bi, si});
       }
    Handle::RecBatch m;
-   size_t off = 0, ac = 0;
+   size_t off = 0;
    for (int c : order) {
       Handle::RecSeg g;
       std::memset(&g, 0, sizeof(g));
@@ -1016,13 +1018,9 @@ static bool merge_recording(Handle *h) {
       g.o_g = off; off = al16(off + (size_t)g.ngroup * sizeof(GroupRec));
       g.o_q = off; off = al16(off + (size_t)g.nqrtt * sizeof(QrttRec));
       g.o_rg = off; off = al16(off + ((size_t)g.nqrtt + 31) / 32 * 4);
-      g.ac_off = ac;
-      ac += ((size_t)g.nprm * h->plans[c & 255].S + 1) & ~(size_t)1;
       m.segs.push_back(g);
    }
-   if (ac > 2 * ac_max) return true;
    if (!ensure(h, m.rec, std::max<size_t>(off, 256), "merged recording")) return false;
-   m.ac_doubles = ac;
    char *dst = (char *)m.rec.p;
    for (size_t k = 0; k < order.size(); k++) {
       const Handle::RecSeg &g = m.segs[k];
@@ -1104,11 +1102,12 @@ static int autotune_impl(Handle *h, int *out) {
    bool seen[256] = {}, alt_p[256] = {}, alt_g[256] = {};
    cudaEvent_t ev[5];
    for (auto &e : ev) cudaEventCreate(&e);
+   int nseg = 0;
    for (size_t bi = 0; bi < h->recs.size() && !h->err; bi++) {
       auto &rb = h->recs[bi];
       char *base = (char *)rb.rec.p;
-      double *ac_half = (double *)h->rec_ac.p + (bi & 1) * ac;
       for (auto &g : rb.segs) {
+         const int wk = replay_worker(h, g.c, nseg++);   // the arena the replay gives this segment
          if (g.c >= kFp32) continue;
          const int c = g.c;
          const ClassPlan &hp = h->plans[c];
@@ -1123,7 +1122,7 @@ static int autotune_impl(Handle *h, int *out) {
          bt.qrtts = (const QrttRec *)(base + g.o_q);
          bt.rowgrp = (const uint32_t *)(base + g.o_rg);
          bt.nprm = g.nprm; bt.nshell = g.nshell; bt.ngroup = g.ngroup; bt.nqrtt = g.nqrtt;
-         bt.AC = ac_half + g.ac_off;
+         bt.AC = (double *)h->rec_ac.p + h->arena_off[wk];
          bt.gscratch = (double *)h->rec_gscr.p;
          seen[c] = true;
          alt_p[c] = prim_has_generated(c);
@@ -1202,9 +1201,6 @@ void libgint_init(void *hh) {
    }
    if (!h->fork_ev) ck(h, cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming), "event");
    if (!h->noalloc_ev) ck(h, cudaEventCreateWithFlags(&h->noalloc_ev, cudaEventDisableTiming), "event");
-   for (auto &row : h->batch_ev)
-      for (cudaEvent_t &e : row)
-         if (!e) ck(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
    for (Slot &s : h->slots) {
       if (!s.ev) ck(h, cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming), "event");
       if (!s.ev_copy) ck(h, cudaEventCreateWithFlags(&s.ev_copy, cudaEventDisableTiming), "event");
@@ -1992,9 +1988,6 @@ void libgint_destroy_handle(void *hh) {
    }
    if (h->fork_ev) cudaEventDestroy(h->fork_ev);
    if (h->noalloc_ev) cudaEventDestroy(h->noalloc_ev);
-   for (auto &row : h->batch_ev)
-      for (cudaEvent_t e : row)
-         if (e) cudaEventDestroy(e);
    if (h->stream) cudaStreamDestroy(h->stream);
    delete h;
 }
