@@ -7,7 +7,7 @@ truncated Coulomb R_c = 6 A, Schwarz 1e-11, seed 0. P is dense (random orbitals)
 set-quartet list grows as N^2: the whole K build holds ~6.4e9 set quartets, 7.2e9 shell quartets
 and 1.05e11 primitive quartets (extrapolated from uniform samples). One step processes a uniform
 sample of 1/stride of its set quartets (--setq-stride, every stride-th ket pair of each bra pair
-from a hashed offset), so that a step takes about a second; the sample is named in
+from a hashed offset; 1/256 by default, 1.3 s per step), and the sample is named in
 config.workload.
 
 One step = one K build over the sample's screened quartet list:
@@ -65,7 +65,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="periodic_l3", choices=sorted(WORKLOADS))
-    ap.add_argument("--setq-stride", type=int, default=512,
+    ap.add_argument("--setq-stride", type=int, default=256,
                     help="process a uniform 1/stride sample of the set quartets (1 = all)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--host-threads", type=int, default=0,
