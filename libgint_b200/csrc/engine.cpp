@@ -816,10 +816,10 @@ static void set_K_impl(Handle *h, int nspin, const double *Ka, const double *Kb,
 // Enqueue one replay of every recorded batch (K zeroed first) on the handle's stream: with
 // kt == nullptr the segments spread over the worker streams (forked from and joined back to the
 // handle's stream), otherwise they run in order on the handle's stream with an event before and
-// after each kernel (kev, kcl: per-kernel timing). ac is the replay AC buffer's half size.
-// eps >= 0: an incremental replay (K is not zeroed; each segment's groups are screened against
+// after each kernel (kev, kcl: per-kernel timing). Each segment's image-summed targets live in
+// its worker stream's arena of the replay AC buffer (prepare_replay). eps >= 0: an incremental replay (K is not zeroed; each segment's groups are screened against
 // eps first, see k_group_screen, and the screened ones skipped).
-static bool enqueue_replay(Handle *h, const DevCtx &ctx, size_t ac, std::vector<cudaEvent_t> *kev,
+static bool enqueue_replay(Handle *h, const DevCtx &ctx, std::vector<cudaEvent_t> *kev,
                            std::vector<int> *kcl, long long *nlaunch, double eps = -1.0) {
    if (eps < 0.0) {
       for (int sp = 0; sp < h->nspin; sp++)
@@ -937,7 +937,7 @@ static double replay_impl(Handle *h, double *kt, double *kcls = nullptr, double 
       std::vector<cudaEvent_t> kev;
       std::vector<int> kcl;
       ck(h, cudaEventRecord(e0, h->stream), "event");
-      enqueue_replay(h, ctx, ac, &kev, &kcl, &h->n_launch, eps);
+      enqueue_replay(h, ctx, &kev, &kcl, &h->n_launch, eps);
       ck(h, cudaEventRecord(e1, h->stream), "event");
       ck(h, cudaEventSynchronize(e1), "replay");
       kt[0] = kt[1] = 0.0;
@@ -962,7 +962,7 @@ static double replay_impl(Handle *h, double *kt, double *kcls = nullptr, double 
          long long n = 0;
          bool ok = ck(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "graph capture");
          if (ok) {
-            ok = enqueue_replay(h, ctx, ac, nullptr, nullptr, &n, eps);
+            ok = enqueue_replay(h, ctx, nullptr, nullptr, &n, eps);
             const cudaError_t ec = cudaStreamEndCapture(h->stream, &graph);
             ok = ok && ck(h, ec, "graph capture");
          }
