@@ -739,13 +739,14 @@ __global__ void __launch_bounds__(256, 4) k_group(DevCtx ctx, BatchArgs bt, int 
    }
 }
 
-// one block of four warps per contraction row, all of them on one workspace (in shared memory, or
+// one block of NT threads per contraction row, all of them on one workspace (in shared memory, or
 // for the largest classes a slice of the global scratch per block): for the classes whose rows are
 // long chains of HRR levels with hundreds to thousands of elements each and which have few rows,
-// a warp per row leaves the GPU mostly idle and takes a level in many rounds. 64 registers: eight
-// blocks per SM
-__global__ void __launch_bounds__(kGroupBlockThreads, 8) k_group_block(DevCtx ctx, BatchArgs bt, int ws_doubles,
-                                                                    int use_global) {
+// a warp per row leaves the GPU mostly idle and takes a level in many rounds. NT = 128 (eight
+// blocks per SM at 64 registers) up to kGroupBlockWideDoubles of workspace, 256 above.
+template <int NT>
+__global__ void __launch_bounds__(NT, 1024 / NT) k_group_block(DevCtx ctx, BatchArgs bt, int ws_doubles,
+                                                                int use_global) {
    extern __shared__ __align__(16) double smem[];
    const ClassPlan *pl = reinterpret_cast<const ClassPlan *>(smem);
    load_plan(bt.plan, smem);
@@ -760,7 +761,7 @@ __global__ void __launch_bounds__(kGroupBlockThreads, 8) k_group_block(DevCtx ct
       const uint32_t gi = row_group_one(bt, q, lane);   // the same in every warp of the block
       if (bt.gflags && !__ldg(bt.gflags + gi)) continue;   // screened on an incremental replay
       const GroupRec G = bt.groups[gi];
-      group_body<kGroupBlockThreads, 1>(ctx, bt, pl, G, q, ws, ws + Hws, (int)threadIdx.x, hrec, kpw);
+      group_body<NT, 1>(ctx, bt, pl, G, q, ws, ws + Hws, (int)threadIdx.x, hrec, kpw);
    }
 }
 
@@ -1009,18 +1010,23 @@ cudaError_t launch_group(const DevCtx &ctx, const BatchArgs &bt, const ClassPlan
    if (bt.fp32) return cudaErrorInvalidValue;   // FP32 segments exist only for classes with k_group3
    const size_t wd = group_warp_doubles(hp);
    if (bt.group_variant == 0 && wd >= (size_t)kGroupBlockMinDoubles) {
+      const bool wide = wd >= (size_t)kGroupBlockWideDoubles;
       const size_t smem = group_hdr_bytes() + (kGroupKpDoubles + wd) * 8;
+      long blocks = 0;
+      int use_global = 0;
+      size_t dyn = smem;
       if (smem <= (size_t)std::min(max_dyn_smem(), 200 * 1024)) {
-         const long blocks = std::max(1L, std::min((long)bt.nqrtt, 148L * 16));
-         k_group_block<<<(unsigned)blocks, kGroupBlockThreads, smem, st>>>(ctx, bt, (int)wd, 0);
-         return cudaGetLastError();
-      }
-      if (bt.gscratch) {   // workspace in the global scratch, which holds group_global_scratch's count
+         blocks = std::max(1L, std::min((long)bt.nqrtt, 148L * 16));
+      } else if (bt.gscratch) {   // workspace in the global scratch, which holds group_global_scratch's count
          int grid = 0, warps = 0;
          group_global_scratch(hp, &grid, &warps);
-         const long blocks = std::max(1L, std::min((long)bt.nqrtt, (long)grid * warps));
-         k_group_block<<<(unsigned)blocks, kGroupBlockThreads, group_hdr_bytes() + kGroupKpDoubles * 8, st>>>(
-            ctx, bt, (int)wd, 1);
+         blocks = std::max(1L, std::min((long)bt.nqrtt, (long)grid * warps));
+         use_global = 1;
+         dyn = group_hdr_bytes() + kGroupKpDoubles * 8;
+      }
+      if (blocks) {
+         if (wide) k_group_block<256><<<(unsigned)blocks, 256, dyn, st>>>(ctx, bt, (int)wd, use_global);
+         else k_group_block<128><<<(unsigned)blocks, 128, dyn, st>>>(ctx, bt, (int)wd, use_global);
          return cudaGetLastError();
       }
    }
@@ -1259,7 +1265,8 @@ cudaError_t preload_kernels() {
    const int smax = max_dyn_smem();
    const void *fns[] = {(const void *)k_prim<1>, (const void *)k_prim<4>, (const void *)k_prim<8>,
                         (const void *)k_prim<32>, (const void *)k_prim2<true>, (const void *)k_prim2<false>,
-                        (const void *)k_group, (const void *)k_group_lane, (const void *)k_group_block};
+                        (const void *)k_group, (const void *)k_group_lane, (const void *)k_group_block<128>,
+                        (const void *)k_group_block<256>};
    for (const void *f : fns)
       if ((e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smax)) != cudaSuccess) return e;
    cudaFuncAttributes a;

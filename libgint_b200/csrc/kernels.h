@@ -76,7 +76,9 @@ size_t group_global_scratch(const ClassPlan &hp, int *grid, int *warps);
 constexpr int kGroupShellCacheDoubles = 16;
 constexpr int kGroupKpDoubles = 32 + kGroupShellCacheDoubles;
 constexpr int kGroupRowsPerWarp = 4;      // consecutive rows a warp of k_group takes at a time
-constexpr int kGroupBlockThreads = 128;   // k_group_block: threads sharing one row's workspace
+// k_group_block: 128 threads share one row's workspace, 256 from this workspace size on (on the
+// 64-molecule l <= 3 workload the wider block was faster from about here on)
+constexpr int kGroupBlockWideDoubles = 6000;
 // k_group_block (variant 0) for the classes whose workspace holds at least this many doubles: on
 // the 64-molecule l <= 3 workload it was faster than one warp per row from about here on
 constexpr int kGroupBlockMinDoubles = 1536;
