@@ -125,7 +125,9 @@ __global__ void __launch_bounds__(128, Group3Shape<LA, LB, LC, LD>::MINB) k_grou
 template <int LA, int LB, int LC, int LD>
 cudaError_t launch_one(const DevCtx &ctx, const BatchArgs &bt, cudaStream_t st) {
    const int threads = 128;
-   const long blocks = std::max(1L, std::min(((long)bt.nqrtt + threads - 1) / threads, 148L * 16));
+   // one 32-row block per warp: rows cost from one primitive to thousands, so the block scheduler,
+   // which starts a new block wherever one finishes, balances them better than a grid-stride loop
+   const long blocks = std::max(1L, std::min(((long)bt.nqrtt + threads - 1) / threads, 1L << 30));
    if constexpr (class_has_fp32(LA, LB, LC, LD)) {
       if (bt.fp32) {
          k_group3<LA, LB, LC, LD, float><<<(unsigned)blocks, threads, 0, st>>>(ctx, bt);
