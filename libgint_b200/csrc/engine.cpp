@@ -1036,20 +1036,29 @@ static bool merge_recording(Handle *h) {
              !cp(g.o_ps + (size_t)pb * 4, s.o_ps, (size_t)s.nprm * 4) ||
              !cp(g.o_sh + (size_t)sb * sizeof(ShellRec), s.o_sh, (size_t)s.nshell * sizeof(ShellRec)) ||
              !cp(g.o_g + (size_t)gb * sizeof(GroupRec), s.o_g, (size_t)s.ngroup * sizeof(GroupRec)) ||
-             !cp(g.o_q + (size_t)qb * sizeof(QrttRec), s.o_q, (size_t)s.nqrtt * sizeof(QrttRec)))
+             !cp(g.o_q + (size_t)qb * sizeof(QrttRec), s.o_q, (size_t)s.nqrtt * sizeof(QrttRec))) {
+            cudaStreamSynchronize(h->stream);   // the copies already queued read the old batches
+            release(m.rec);
             return false;
+         }
          if ((pb || sb || gb || qb) &&
              !ck(h, launch_rebase_part((uint32_t *)(dst + g.o_ps) + pb, s.nprm, (ShellRec *)(dst + g.o_sh) + sb,
                                        s.nshell, (GroupRec *)(dst + g.o_g) + gb, s.ngroup, pb, sb, gb, qb, h->stream),
-                 "merged recording rebase"))
+                 "merged recording rebase")) {
+            cudaStreamSynchronize(h->stream);
+            release(m.rec);
             return false;
+         }
          pb += s.nprm; sb += s.nshell; gb += s.ngroup; qb += s.nqrtt;
       }
       if (!ck(h, launch_row_groups((const GroupRec *)(dst + g.o_g), g.ngroup, (uint32_t *)(dst + g.o_rg), h->stream),
-              "merged recording row table"))
+              "merged recording row table")) {
+         cudaStreamSynchronize(h->stream);
+         release(m.rec);
          return false;
+      }
    }
-   if (!ck(h, cudaStreamSynchronize(h->stream), "merged recording")) return false;
+   if (!ck(h, cudaStreamSynchronize(h->stream), "merged recording")) { release(m.rec); return false; }
    for (auto &rb : h->recs) { release(rb.rec); release(rb.gbuf); }
    h->recs.clear();
    h->recs.push_back(m);
